@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""Benchmark of the R-tree build / join / overlay path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the R-tree build-and-query configuration): 10M axis-aligned float32
+boxes around a 64-Gaussian mixture (sigma 0.02), widths/heights exponential
+with mean 1e-4, seed = rank.  A step = one bottom-up bulk load at fanout 16
+(MORTON32 keys of box centres -> onesweep radix sort -> level packing) of the
+whole 10M-box array; `value` = boxes of all ranks / max-over-ranks device time
+per step, in Mboxes/s.  Inputs (160 MB) are larger than the 126 MB L2 and L2
+is also flushed (256 MB write) between timed steps.
+
+Reported beside it (same JSON line): the other builds of that configuration
+(bottom-up/top-down at fanout 16 and 32), 1M window queries (side uniform
+1e-4..1e-2) joined against the fanout-16 tree, and the small overlay
+configuration (2 x 10,000 stars, 8-32 vertices, radius log-uniform 1e-3..1e-2)
+clipped with the plain and the batched schedule.
+
+--impl reference times the reference's own CPU build (BotomUp-rtree.cu:776-833,
+qsort + packing, built from its sources into oracle/_ref) on the same boxes
+quantised to int64 (round(v * 1e6)), a bounded sample per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_BOXES = 10_000_000
+N_WINDOWS = 1_000_000
+FANOUT = 16
+METRIC = "overlay pairs/s & R-tree build Mboxes/s on 1 B200; batched+grad vs plain"
+WORKLOAD = "rtree_build_10M_f32_mixture64_bottomup_f16_morton32"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def time_steps(fn, steps, warmup, flush, world, before=None, after=None):
+    """Runs warmup + steps; returns per-step device ms (CUDA events on the
+    current stream, L2 flushed between steps) and the bracketed wall time."""
+    import torch
+
+    for _ in range(warmup):
+        r = fn()
+        if after:
+            after(r)
+    torch.cuda.synchronize()
+    ms = []
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        flush()
+        if before:
+            before()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        r = fn()
+        b.record()
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+        if after:
+            after(r)
+    barrier(world)
+    torch.cuda.synchronize()
+    return ms, time.perf_counter() - t0
+
+
+def reference_cpu_build(rects: np.ndarray) -> float:
+    """The reference's CPU bottom-up build (qsort + packing) on rects; returns ms."""
+    import oracle
+
+    res = oracle.ref_bu_run(rects, FANOUT, query=False)
+    return float(res["ms"][0])
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    from parlllelrtree_b200 import datagen as dg
+
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's CPU code) is not built"}))
+        return
+    sample = 2_000_000
+    rects = dg.quantise(dg.mixture_boxes(N_BOXES, seed=0))
+    for _ in range(args.warmup):
+        reference_cpu_build(rects[:sample])
+    ms = [reference_cpu_build(rects[i * 997 % (N_BOXES - sample):][:sample]) for i in range(args.steps)]
+    mean = float(np.mean(ms))
+    v = sample / (mean * 1e-3) / 1e6
+    print(json.dumps({
+        "metric": METRIC, "impl": "reference", "value": v, "unit": "Mboxes/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_boxes": N_BOXES, "fanout": FANOUT,
+                   "sample_boxes_per_step": sample, "coords": "int64 round(v*1e6)"},
+        "cpu_baseline": {"value": v, "unit": "Mboxes/s", "cores": 1, "kind": "reference",
+                         "sample": f"{sample} of the {N_BOXES} boxes per step, qsort + packing "
+                                   "(BotomUp-rtree.cu:776-833) as written, single thread"},
+        "e2e": {"value": v, "unit": "Mboxes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_ours(args):
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import parlllelrtree_b200 as prt
+    from parlllelrtree_b200 import _lib
+    from parlllelrtree_b200 import datagen as dg
+
+    boxes_h = dg.mixture_boxes(N_BOXES, seed=rank)
+    boxes = torch.from_numpy(boxes_h).cuda()
+    boxes_pin = torch.from_numpy(boxes_h).pin_memory()
+    flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def flush():
+        flush_buf.zero_()
+
+    def step():
+        return prt.build_bottomup(boxes, fanout=FANOUT, key_mode="morton32")
+
+    def drop(t):
+        del t
+
+    # main timed region: profiled launches, clocks sampled
+    _lib.profile_enable(False)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    _lib.profile_reset()
+    _lib.profile_enable(True)
+    with ClockSampler(local) as clk:
+        ms, wall = time_steps(step, args.steps, 0, flush, world)
+    _lib.profile_enable(False)
+    prof = _lib.profile_read()
+    _lib.profile_reset()
+    mean_ms = float(np.mean(ms))
+    t_max = max_over_ranks(mean_ms, world)
+    value = N_BOXES * world / (t_max * 1e-3) / 1e6
+
+    # end to end through the public API: pinned host boxes -> device -> build
+    # -> top level read back
+    def step_e2e():
+        d = boxes_pin.to("cuda", non_blocking=True)
+        t = prt.build_bottomup(d, fanout=FANOUT, key_mode="morton32")
+        top = t.level_mbr(t.levels - 1)
+        return t, top
+
+    ms_e2e, _ = time_steps(step_e2e, args.steps, 1, flush, world)
+    t_e2e = max_over_ranks(float(np.mean(ms_e2e)), world)
+    e2e = N_BOXES * world / (t_e2e * 1e-3) / 1e6
+    top_levels = prt.build_bottomup(boxes, fanout=FANOUT).level_counts[-1]
+
+    # roofline of the dominant kernel
+    total = sum(v[0] for v in prof.values()) or 1.0
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    peak, peak_kind = hbm_peak()
+    dom_name, (dom_ms, dom_n) = dom
+    per_launch_ms = dom_ms / max(dom_n, 1)
+    algo_bytes = {
+        # one radix pass moves every (key, value): read 4 + 4 B, write 4 + 4 B
+        "onesweep_pass": 16 * N_BOXES,
+        # gather of a 16 B box by index + 4 B index read + 16 B entry + 4 B id
+        # + 4 B leaf perm writes
+        "pack_leaf": 44 * N_BOXES,
+        "morton32": 24 * N_BOXES,
+        "hist": 4 * N_BOXES,
+    }.get(dom_name)
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic_per_launch.json")
+    if os.path.exists(tf):
+        try:
+            with open(tf) as f:
+                traffic = json.load(f).get(f"{WORKLOAD}:{dom_name}")
+        except Exception:
+            traffic = None
+    roofline = None
+    if algo_bytes:
+        achieved = algo_bytes / (per_launch_ms * 1e-3) / 1e9
+        roofline = {"kernel": dom_name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                    "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": per_launch_ms}
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "Mboxes/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_boxes_per_gpu": N_BOXES, "fanout": FANOUT, "key_mode": "morton32",
+                   "l2": "inputs (160 MB) larger than L2; 256 MB L2 flush between timed steps",
+                   "parallelism": f"replicas x{world} (independent box sets, no collective)"},
+        "e2e": {"value": e2e, "unit": "Mboxes/s", "h2d_bytes_per_step": int(boxes_h.nbytes),
+                "d2h_bytes_per_step": int(top_levels * 32)},
+        "gpu_launches": int(sum(v[1] for v in prof.values())),
+        "kernel_share": {k: round(v[0] / total, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+        "roofline": roofline,
+        "clocks": clk.summary(),
+        "wall_s_timed": wall,
+    }
+
+    if rank == 0 and not args.no_extras:
+        out["secondary"] = secondary(prt, boxes, flush, world)
+        # CPU baseline: the reference's own CPU build on a bounded sample
+        sample = N_BOXES
+        rects = dg.quantise(boxes_h[:sample])
+        try:
+            cms = reference_cpu_build(rects)
+            out["cpu_baseline"] = {"value": sample / (cms * 1e-3) / 1e6, "unit": "Mboxes/s", "cores": 1,
+                                   "kind": "reference",
+                                   "sample": f"all {sample} boxes quantised to int64, one qsort + packing pass "
+                                             "(BotomUp-rtree.cu:776-833) as written"}
+        except Exception as e:  # oracle/_ref missing
+            out["cpu_baseline"] = {"value": None, "unit": "Mboxes/s", "cores": 1, "kind": "reference",
+                                   "sample": f"unavailable: {e}"}
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def secondary(prt, boxes, flush, world):
+    """Other builds of the configuration, the 1M-window join and the small
+    overlay configuration, each timed with CUDA events (median of 5)."""
+    import torch
+    from parlllelrtree_b200 import datagen as dg
+
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(reps):
+            flush()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            r = fn()
+            b.record()
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+            del r
+        return float(np.median(ms))
+
+    res = {}
+    n = len(boxes)
+    for name, fn in (("bottomup_f16", lambda: prt.build_bottomup(boxes, 16)),
+                     ("bottomup_f32", lambda: prt.build_bottomup(boxes, 32)),
+                     ("topdown_f16", lambda: prt.build_topdown(boxes, 16)),
+                     ("topdown_f32", lambda: prt.build_topdown(boxes, 32))):
+        ms = timed(fn)
+        res[f"build_{name}_mboxes_s"] = n / (ms * 1e-3) / 1e6
+    tree = prt.build_bottomup(boxes, 16)
+    win = torch.from_numpy(dg.window_queries(N_WINDOWS, seed=1)).cuda()
+    npairs = len(tree.join(win))
+    cap = npairs + 1024
+    out = torch.empty((cap, 2), dtype=torch.int32, device="cuda")
+    import ctypes as C
+
+    from parlllelrtree_b200 import _lib
+
+    cnt = C.c_int64(0)
+
+    def join():
+        _lib.check(_lib.lib().prt_join(tree._h, C.c_void_p(win.data_ptr()), tree.coord, len(win),
+                                       C.c_void_p(out.data_ptr()), cap, C.byref(cnt),
+                                       C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        return cnt.value
+
+    ms = timed(join)
+    res["join_1M_windows_queries_s"] = N_WINDOWS / (ms * 1e-3)
+    res["join_1M_windows_pairs_s"] = npairs / (ms * 1e-3)
+    res["join_1M_windows_pairs"] = npairs
+
+    # small overlay configuration: 2 x 10,000 stars
+    A = dg.star_layer(10000, seed=0)
+    B = dg.star_layer(10000, seed=1)
+    LA, LB = prt.Layer.from_dict(A), prt.Layer.from_dict(B)
+    t = prt.build_bottomup(LA.mbr(), fanout=16)
+    pairs = t.join(LB.mbr())
+    l2p = t.leaf_order()
+    res["overlay_small_pairs"] = len(pairs)
+    for sched in ("plain", "batched"):
+        ms = timed(lambda: prt.overlay(pairs, LA, LB, leaf_to_poly=l2p, sched=sched))
+        res[f"overlay_small_{sched}_pairs_s"] = len(pairs) / (ms * 1e-3)
+    ms = timed(lambda: prt.intersection_area(LA, LB, torch.arange(10000, device="cuda"),
+                                             torch.arange(10000, device="cuda")))
+    res["area_fwd_10k_pairs_s"] = 10000 / (ms * 1e-3)
+    return res
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

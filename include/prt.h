@@ -1,0 +1,249 @@
+/* prt.h — C ABI of the B200 filter-and-refine spatial join and polygon overlay.
+ *
+ * Drop-in for the R-tree / overlay path of ParlllelRtree.  Every entry point
+ * takes plain pointers and sizes; device pointers are named d_*, host
+ * pointers h_*; `stream` is a cudaStream_t passed as void* (NULL = default
+ * stream).  Every call returns a status (PRT_OK = 0); prt_last_error() gives a
+ * thread-local message for the last failure.  The library never exits the
+ * process and never falls back to the CPU: without a usable CUDA device every
+ * compute call returns PRT_ERR_CUDA.
+ *
+ * Reference interfaces replaced (file:line in the reference project):
+ *   prt_build_bottomup   CalcuateZOrderValue + LocalSort/scan1/scan2/Reorder +
+ *                        Construction_init/Construction1 and their host loop
+ *                        (BotomUp-rtree.cu:73-266, 373-426, 756-874)
+ *   prt_build_topdown    changeX/changeY + fun, prefix*, sort + fun/fun1/fun2
+ *                        (TopDown-rtree.cu:162-353, 465-481, 504-524, 629-687)
+ *   prt_tree_export_bu   the rtree_node array the BU program copies back
+ *                        (BotomUp-rtree.cu:47-54, 890)
+ *   prt_tree_export_td   nodes_index / nodes_mbr slot arrays
+ *                        (TopDown-rtree.cu:15-20, 689-690)
+ *   prt_tree_leaf_order  the leaf-order -> record remap zOrder[].index used by
+ *                        Execute (vector_map_overlay_gpc_kernel.cu:89)
+ *   prt_join             init + query1 BFS batches (BotomUp-rtree.cu:592-630,
+ *                        914-987; TopDown-rtree.cu:355-377, 450-463, 694-758),
+ *                        emitting the rtree_search {nodeid, queryid} pairs the
+ *                        overlay consumes (vector_map_overlay_gpc_kernel.cu:89-90)
+ *   prt_query_counts     RtreeSearch / RtreeSearchHelp counters
+ *                        (BotomUp-rtree.cu:439-483, TopDown-rtree.cu:56-76)
+ *   prt_overlay_run      run() + Execute + gpc_polygon_clip
+ *                        (vector_map_overlay_gpc_kernel.cu:61-750)
+ *   prt_results_*        the gpc_polygon result array of run()
+ *                        (vector_map_overlay_gpc_kernel.cu:64-65, 698-741)
+ *   prt_clip_pair_host   gpc_polygon_clip on one host pair (for tests; the
+ *                        clip still runs on the device)
+ */
+#ifndef PRT_H
+#define PRT_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define PRT_OK 0
+#define PRT_ERR_INVALID 1  /* bad argument */
+#define PRT_ERR_CAPACITY 2 /* an output buffer was too small; counts are still reported */
+#define PRT_ERR_TIMEOUT 3  /* a bounded device-side wait gave up */
+#define PRT_ERR_CUDA 4     /* CUDA runtime error (or no device) */
+#define PRT_ERR_NOMEM 5    /* device allocation failed */
+
+/* ---- box coordinate types: boxes are (x1, y1, x2, y2) per record ---- */
+#define PRT_COORD_I64 0 /* int64, the reference's bounding_box.rect / MBR */
+#define PRT_COORD_F32 1
+#define PRT_COORD_F64 2
+#define PRT_COORD_I32 3 /* the overlay's quantised MBRs */
+
+/* ---- bottom-up key modes ---- */
+#define PRT_KEY_REF64 0    /* the reference's 4-D corner interleave (int64 boxes only) */
+#define PRT_KEY_MORTON32 1 /* 2-D Morton code of box centres on a 65536^2 grid */
+
+#define PRT_BOTTOM_UP 0
+#define PRT_TOP_DOWN 1
+
+/* ---- GPC operations (the reference hard-codes intersection) ---- */
+#define PRT_GPC_DIFF 0
+#define PRT_GPC_INT 1
+#define PRT_GPC_XOR 2
+#define PRT_GPC_UNION 3
+
+/* ---- overlay schedules ---- */
+#define PRT_SCHED_PLAIN 0   /* one thread per pair, pairs in input order */
+#define PRT_SCHED_BATCHED 1 /* size-binned pairs, persistent work-stealing launch */
+
+#define PRT_MAX_LEVELS 40
+
+typedef struct prt_tree prt_tree;
+typedef struct prt_results prt_results;
+
+/* Candidate pair: leaf entry position (the reference's nodeid - offset) and
+ * query record id (vector_map_overlay_gpc_kernel.cu:89-90). */
+typedef struct {
+  int32_t nodeid;
+  int32_t queryid;
+} prt_pair;
+
+const char *prt_last_error(void);
+int prt_version(void);
+/* Number of CUDA devices visible to the library (0 when none). */
+int prt_device_count(void);
+
+/* ---------------------------------------------------------------- build */
+
+/* Bulk-loads an R-tree bottom-up: keys (key_mode) -> stable radix sort ->
+ * leaves of `fanout` consecutive records -> each upper level groups `fanout`
+ * consecutive nodes; root = the single node of the top level.
+ * d_boxes: n records of 4 coordinates (coord_type); d_ids: optional record ids
+ * stored in the leaves (NULL = 0..n-1).  fanout in [2, 32]. */
+int prt_build_bottomup(const void *d_boxes, int coord_type, const int32_t *d_ids, int64_t n,
+                       int fanout, int key_mode, void *stream, prt_tree **out);
+
+/* Bulk-loads an R-tree top-down: with H node levels, level p = 0..H-1 stably
+ * sorts every run of fanout^(H-p) consecutive records by x1 (p even) or y1
+ * (p odd), then packs like the bottom-up build. */
+int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids, int64_t n,
+                      int fanout, void *stream, prt_tree **out);
+
+int prt_tree_free(prt_tree *t);
+
+/* info[0] n, [1] fanout, [2] levels L (level 0 = records), [3] kind,
+ * [4] coord type, [5] key mode, [8 + l] entries at level l (l < L).
+ * `info` holds at least 8 + PRT_MAX_LEVELS int64. */
+int prt_tree_info(const prt_tree *t, int64_t *info);
+
+/* Entry boxes of one level, converted to double (exact for float32, float64
+ * and integers below 2^53), n_l x 4 into host memory. */
+int prt_tree_level_mbr(const prt_tree *t, int level, double *h_out);
+
+/* Record id (d_ids[i], or i) of every leaf entry in leaf order: the zOrder
+ * remap; n int32 into device memory. */
+int prt_tree_leaf_order(const prt_tree *t, int32_t *d_out, void *stream);
+
+/* The reference's bottom-up node array (BotomUp-rtree.cu:47-54): leaves
+ * first, root last; per node flag (0 leaf, 1 internal), num, mbr[fanout][4]
+ * (as double), children[fanout] (node index, -1 in leaves), data[fanout]
+ * (record id, -1 in internal nodes).  Host buffers sized by
+ * prt_tree_export_bu_size(). */
+int prt_tree_export_bu_size(const prt_tree *t, int64_t *n_nodes);
+int prt_tree_export_bu(const prt_tree *t, int32_t *h_flag, int32_t *h_num, double *h_mbr,
+                       int32_t *h_children, int32_t *h_data, int32_t *h_root);
+
+/* The reference's top-down slot arrays (TopDown-rtree.cu:504-524, 575-624):
+ * root slots first; nodes_index > 0 is the child's first slot, < 0 is
+ * -(leaf position)-1, 0 is empty; nodes_mbr (x1, y1, x2, y2) as double, zero
+ * for empty slots.  offsets: the level offset vector (n_levels + 1 values). */
+int prt_tree_export_td_size(const prt_tree *t, int64_t *n_slots, int32_t *n_offsets);
+int prt_tree_export_td(const prt_tree *t, int32_t *h_nodes_index, double *h_nodes_mbr,
+                       int32_t *h_offsets);
+
+/* ---------------------------------------------------------------- join */
+
+/* All (leaf entry, query) pairs whose boxes intersect (closed intervals: boxes
+ * that touch intersect, as the reference's Overlap).  Breadth-first over the
+ * levels for all queries at once.  Writes up to `cap` pairs to d_pairs in no
+ * particular order and the total count to *h_count; returns
+ * PRT_ERR_CAPACITY (count still exact) when cap is too small. */
+int prt_join(const prt_tree *t, const void *d_queries, int coord_type, int64_t nq,
+             prt_pair *d_pairs, int64_t cap, int64_t *h_count, void *stream);
+
+/* Same, with the pairs sorted by (queryid, nodeid). */
+int prt_join_sorted(const prt_tree *t, const void *d_queries, int coord_type, int64_t nq,
+                    prt_pair *d_pairs, int64_t cap, int64_t *h_count, void *stream);
+
+/* Per-query counters of the reference's DFS search, d_counts nq x 3 int64:
+ * entries examined (node fill, or fanout per node when td_slots != 0 as the
+ * top-down program counts), sum over visited nodes of max(0, overlapping
+ * entries - 1) (the RtreeSearch return value), overlapping leaf entries. */
+int prt_query_counts(const prt_tree *t, const void *d_queries, int coord_type, int64_t nq,
+                     int td_slots, int64_t *d_counts, void *stream);
+
+/* ---------------------------------------------------------------- overlay */
+
+/* A polygon layer in device memory (ring CSR):
+ *   poly_ring[P+1]  ring offsets per polygon
+ *   ring_vert[R+1]  vertex offsets per ring
+ *   ring_hole[R]    hole flag per ring (informational; the clip uses even-odd parity)
+ *   xy[V]           vertices (x, y) as double pairs */
+typedef struct {
+  const int64_t *poly_ring;
+  const int64_t *ring_vert;
+  const int32_t *ring_hole;
+  const double *xy;
+  int64_t n_poly;
+} prt_layer;
+
+/* Clips every pair: subject = base polygon leaf_to_poly[nodeid - offset]
+ * (or nodeid - offset when leaf_to_poly is NULL), clip = overlay polygon
+ * queryid, with GPC semantics for `op`.  The result set (one gpc_polygon per
+ * pair, device resident) is returned in *out.  sched: PRT_SCHED_*. */
+int prt_overlay_run(const prt_pair *d_pairs, int64_t n_pairs, int32_t offset,
+                    const int32_t *d_leaf_to_poly, const prt_layer *base, const prt_layer *overlay,
+                    int op, int sched, void *stream, prt_results **out);
+
+/* The reference's single-contour CSR (readData, vector_map_overlay_gpc_kernel.cu:752-888):
+ * num[] vertex count, prefix[] first vertex (int64), vertex[] (x, y) doubles,
+ * hole[] flag, per polygon. */
+int prt_overlay_run_ref(const prt_pair *d_pairs, int64_t n_pairs, int32_t offset,
+                        const int32_t *d_leaf_to_poly,
+                        const int32_t *d_num_base, const int64_t *d_prefix_base,
+                        const double *d_vertex_base, const int32_t *d_hole_base, int64_t n_base,
+                        const int32_t *d_num_overlay, const int64_t *d_prefix_overlay,
+                        const double *d_vertex_overlay, const int32_t *d_hole_overlay,
+                        int64_t n_overlay, int op, int sched, void *stream, prt_results **out);
+
+/* sizes[0] pairs, [1] contours, [2] vertices, [3] non-empty results,
+ * [4] pairs retried with larger arenas. */
+int prt_results_sizes(const prt_results *r, int64_t *sizes);
+/* Device views of the result arrays (valid until prt_results_free).  Like the
+ * reference's gpc_polygon array, each pair points at its own contours:
+ * pair i owns contours [pair_cont_start[i], + pair_ncont[i]); contour c owns
+ * vertices [cont_vert_start[c], + cont_nverts[c]) of xy (x, y pairs). */
+int prt_results_device(const prt_results *r, const int64_t **pair_cont_start,
+                       const int32_t **pair_ncont, const int64_t **cont_vert_start,
+                       const int32_t **cont_nverts, const int32_t **cont_hole, const double **xy);
+/* Copies the results to host buffers in pair order (CSR): h_pair_cont_off
+ * [pairs+1], h_cont_nverts / h_cont_hole [contours], h_xy [2*vertices]. */
+int prt_results_copy(const prt_results *r, int64_t *h_pair_cont_off, int32_t *h_cont_nverts,
+                     int32_t *h_cont_hole, double *h_xy);
+/* Per-pair intersection area of the results (hole contours negative). */
+int prt_results_area(const prt_results *r, double *d_area, void *stream);
+int prt_results_free(prt_results *r);
+
+/* One pair from host memory (rings as counts + packed xy), clipped on the
+ * device; the result is written to host buffers.  Returns PRT_ERR_CAPACITY
+ * (with *out_ncont / *out_nv set) when cont_cap / vert_cap are too small. */
+int prt_clip_pair_host(int op, int s_ncont, const int32_t *s_nverts, const double *s_xy,
+                       int c_ncont, const int32_t *c_nverts, const double *c_xy,
+                       int32_t *out_ncont, int32_t cont_cap, int32_t *out_nverts,
+                       int32_t *out_hole, int64_t *out_nv, int64_t vert_cap, double *out_xy);
+
+/* ---------------------------------------------------------------- area + adjoint */
+
+/* Intersection area of each pair (subject = base polygon pair_a[i], clip =
+ * overlay polygon pair_b[i]) and its gradient with respect to every vertex:
+ *   prt_area_fwd: d_area[i] = area(A_i ∩ B_i) (GPC clip + shoelace)
+ *   prt_area_bwd: d_grad_base / d_grad_overlay (V x 2 doubles, accumulated
+ *                 with += over pairs; zero them first) += d_upstream[i] *
+ *                 d area_i / d vertex, recomputing the boundary pieces. */
+int prt_area_fwd(const int32_t *d_pair_a, const int32_t *d_pair_b, int64_t n_pairs,
+                 const prt_layer *base, const prt_layer *overlay, double *d_area, void *stream);
+int prt_area_bwd(const int32_t *d_pair_a, const int32_t *d_pair_b, int64_t n_pairs,
+                 const prt_layer *base, const prt_layer *overlay, const double *d_upstream,
+                 double *d_grad_base, double *d_grad_overlay, void *stream);
+
+/* ---------------------------------------------------------------- profiling */
+
+/* Kernel launch profiler (no reference counterpart): when enabled, every
+ * library kernel launch is bracketed by CUDA events on its stream.
+ * prt_profile_read returns the number of kernel names (up to cap) and writes
+ * newline-separated names, summed device milliseconds and launch counts. */
+int prt_profile_enable(int on);
+int prt_profile_reset(void);
+int prt_profile_read(char *names, int names_cap, double *ms_total, int64_t *launches, int cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,291 @@
+// Breadth-first batched join: every query descends the tree level by level,
+// all queries at once.  A frontier item is (query, node); a group of G lanes
+// (G = fanout rounded up to a power of two) tests the node's entries against
+// the query box, a warp ballot compacts the hits, and one atomicAdd per warp
+// reserves their slots in the next frontier (or, at the leaf level, in the
+// pair output).  Frontier counts stay on the device and every launch
+// grid-strides over the current count, so a whole join is a fixed sequence of
+// launches with no host round trip until the final count is read.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "prt_internal.cuh"
+
+namespace prt {
+namespace {
+
+constexpr int kJoinBlock = 256;
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+struct JoinLevel {
+  const void *mbr;          // entries of node level l (Box<T>)
+  int64_t n_entries;        // entries at level l
+  const uint2 *in;          // frontier (query, node); nullptr = (q, 0) for all queries
+  const unsigned long long *in_count;
+  int64_t in_cap;
+  uint2 *out;               // next frontier, or pairs at the leaf level
+  unsigned long long *out_count;
+  int64_t out_cap;
+  int leaf;                 // 1: emit (entry, query) pairs
+  int64_t nq;
+  long long *counts;        // optional per-query reference counters
+  int td_slots;
+};
+
+template <typename T, int G>
+__global__ void __launch_bounds__(kJoinBlock) expand_kernel(JoinLevel J, const Box<T> *__restrict__ queries,
+                                                            int fanout) {
+  const Box<T> *mbr = reinterpret_cast<const Box<T> *>(J.mbr);
+  const int lane = threadIdx.x & 31;
+  const int sub = lane / G;           // group within the warp
+  const int e = lane % G;             // entry within the node
+  constexpr int kGroups = 32 / G;
+  const uint32_t gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (sub * G));
+  int64_t count = J.in ? (int64_t)min((unsigned long long)J.in_cap, *J.in_count) : J.nq;
+  const int64_t warp_id = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t wb = warp_id * kGroups; wb < count; wb += n_warps * kGroups) {
+    const int64_t item = wb + sub;
+    bool live = item < count;
+    uint32_t q = 0, node = 0;
+    if (live) {
+      if (J.in) {
+        uint2 it = J.in[item];
+        q = it.x;
+        node = it.y;
+      } else {
+        q = (uint32_t)item;
+      }
+    }
+    const int64_t entry = (int64_t)node * fanout + e;
+    bool hit = false;
+    if (live && e < fanout) {
+      Box<T> qb = load_box(queries, q);
+      Box<T> eb = load_box(mbr, entry);  // padded slots hold a box that intersects nothing
+      hit = overlaps(eb, qb);
+    }
+    const uint32_t ballot = __ballot_sync(0xffffffffu, hit);
+    if (J.counts && live && e == 0) {
+      int k = __popc(ballot & gmask);
+      int64_t fill = J.td_slots ? fanout : min((int64_t)fanout, J.n_entries - (int64_t)node * fanout);
+      atomicAdd(reinterpret_cast<unsigned long long *>(&J.counts[3 * (int64_t)q]), (unsigned long long)fill);
+      if (k > 1) atomicAdd(reinterpret_cast<unsigned long long *>(&J.counts[3 * (int64_t)q + 1]),
+                           (unsigned long long)(k - 1));
+      if (J.leaf && k) atomicAdd(reinterpret_cast<unsigned long long *>(&J.counts[3 * (int64_t)q + 2]),
+                                 (unsigned long long)k);
+    }
+    if (!ballot) continue;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(J.out_count, (unsigned long long)__popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (hit) {
+      unsigned long long slot = base + __popc(ballot & lanemask_lt());
+      if ((int64_t)slot < J.out_cap) {
+        J.out[slot] = J.leaf ? make_uint2((uint32_t)entry, q) : make_uint2(q, (uint32_t)entry);
+      }
+    }
+  }
+}
+
+template <typename T>
+int launch_expand(const JoinLevel &J, const void *queries, int fanout, cudaStream_t s) {
+  const Box<T> *q = reinterpret_cast<const Box<T> *>(queries);
+  int blocks = kSMs * 8;
+  if (fanout <= 2) {
+    PRT_PROF("expand", s);
+    expand_kernel<T, 2><<<blocks, kJoinBlock, 0, s>>>(J, q, fanout);
+  }
+  else if (fanout <= 4) {
+    PRT_PROF("expand", s);
+    expand_kernel<T, 4><<<blocks, kJoinBlock, 0, s>>>(J, q, fanout);
+  }
+  else if (fanout <= 8) {
+    PRT_PROF("expand", s);
+    expand_kernel<T, 8><<<blocks, kJoinBlock, 0, s>>>(J, q, fanout);
+  }
+  else if (fanout <= 16) {
+    PRT_PROF("expand", s);
+    expand_kernel<T, 16><<<blocks, kJoinBlock, 0, s>>>(J, q, fanout);
+  }
+  else {
+    PRT_PROF("expand", s);
+    expand_kernel<T, 32><<<blocks, kJoinBlock, 0, s>>>(J, q, fanout);
+  }
+  return PRT_OK;
+}
+
+// Frontier capacity that worked last time (grows across calls).
+int64_t g_frontier_hint = 1 << 20;
+
+// Runs the traversal.  pairs may be nullptr with cap 0 (count only).
+int run_join(const prt_tree *t, const void *d_queries, int coord, int64_t nq, uint2 *d_pairs, int64_t cap,
+             int64_t *h_count, long long *d_counts, int td_slots, cudaStream_t s) {
+  PRT_CHECK(t != nullptr, PRT_ERR_INVALID, "tree is NULL");
+  PRT_CHECK(coord == t->coord, PRT_ERR_INVALID, "query coordinate type %d differs from the tree's %d", coord,
+            t->coord);
+  PRT_CHECK(nq >= 0 && nq < (1ll << 31), PRT_ERR_INVALID, "nq=%lld", (long long)nq);
+  PRT_CHECK(cap >= 0, PRT_ERR_INVALID, "cap < 0");
+  if (h_count) *h_count = 0;
+  if (nq == 0) return PRT_OK;
+  const TreeLevels &L = t->lv;
+  const size_t bs = 4 * coord_size(t->coord);
+  int64_t fcap = std::max<int64_t>(g_frontier_hint, 4 * nq);
+  for (int attempt = 0; attempt < 8; attempt++) {
+    unsigned long long *cnt = nullptr;
+    uint2 *fr[2] = {nullptr, nullptr};
+    int rc = dalloc(&cnt, PRT_MAX_LEVELS + 2, s);
+    if (!rc && L.levels > 1) rc = dalloc(&fr[0], fcap, s);
+    if (!rc && L.levels > 2) rc = dalloc(&fr[1], fcap, s);
+    if (!rc) {
+      cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * (PRT_MAX_LEVELS + 2), s);
+      if (e != cudaSuccess) rc = cuda_status(e, "memset");
+    }
+    if (!rc && d_counts) {
+      cudaError_t e = cudaMemsetAsync(d_counts, 0, sizeof(long long) * 3 * nq, s);
+      if (e != cudaSuccess) rc = cuda_status(e, "memset");
+    }
+    // level L-1 (root node) down to 0
+    int cur = -1;
+    for (int l = L.levels - 1; l >= 0 && !rc; l--) {
+      JoinLevel J;
+      J.mbr = reinterpret_cast<const char *>(t->d_mbr) + L.offset[l] * bs;
+      J.n_entries = L.count[l];
+      J.in = cur < 0 ? nullptr : fr[cur];
+      J.in_count = cur < 0 ? nullptr : &cnt[l + 1];
+      J.in_cap = fcap;
+      J.leaf = l == 0;
+      int nxt = cur < 0 ? 0 : 1 - cur;
+      J.out = J.leaf ? d_pairs : fr[nxt];
+      J.out_count = J.leaf ? &cnt[PRT_MAX_LEVELS] : &cnt[l];
+      J.out_cap = J.leaf ? cap : fcap;
+      J.nq = nq;
+      J.counts = d_counts;
+      J.td_slots = td_slots;
+      rc = dispatch_coord(t->coord, [&](auto tag) {
+        using T = decltype(tag);
+        return launch_expand<T>(J, d_queries, t->fanout, s);
+      });
+      cur = nxt;
+    }
+    if (!rc) {
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) rc = cuda_status(e, "join launch");
+    }
+    std::vector<unsigned long long> h(PRT_MAX_LEVELS + 2, 0);
+    if (!rc) {
+      cudaError_t e = cudaMemcpyAsync(h.data(), cnt, sizeof(unsigned long long) * (PRT_MAX_LEVELS + 2),
+                                      cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) rc = cuda_status(e, "join");
+    }
+    dfree(cnt, s);
+    dfree(fr[0], s);
+    dfree(fr[1], s);
+    if (rc) return rc;
+    unsigned long long worst = 0;
+    for (int l = 1; l < L.levels; l++) worst = std::max(worst, h[l]);
+    if ((int64_t)worst > fcap) {
+      fcap = (int64_t)(worst + worst / 4 + 1024);
+      g_frontier_hint = std::max(g_frontier_hint, fcap);
+      continue;
+    }
+    int64_t np = (int64_t)h[PRT_MAX_LEVELS];
+    if (h_count) *h_count = np;
+    if (np > cap && d_pairs) {
+      set_error("join: %lld pairs exceed capacity %lld", (long long)np, (long long)cap);
+      return PRT_ERR_CAPACITY;
+    }
+    return PRT_OK;
+  }
+  set_error("join: frontier kept overflowing");
+  return PRT_ERR_CAPACITY;
+}
+
+__global__ void pair_key_kernel(const uint2 *__restrict__ p, int64_t n, uint64_t *__restrict__ k,
+                                uint32_t *__restrict__ v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint2 x = p[i];
+    k[i] = ((uint64_t)x.y << 32) | x.x;
+    v[i] = x.x;
+  }
+}
+
+__global__ void pair_unkey_kernel(const uint64_t *k0, const uint64_t *k1, const int *sel, int64_t n,
+                                  uint2 *__restrict__ p) {
+  const uint64_t *k = *sel ? k1 : k0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t x = k[i];
+    p[i] = make_uint2((uint32_t)x, (uint32_t)(x >> 32));
+  }
+}
+
+}  // namespace
+}  // namespace prt
+
+using namespace prt;
+
+extern "C" {
+
+int prt_join(const prt_tree *t, const void *d_queries, int coord_type, int64_t nq, prt_pair *d_pairs, int64_t cap,
+             int64_t *h_count, void *stream) {
+  return run_join(t, d_queries, coord_type, nq, reinterpret_cast<uint2 *>(d_pairs), d_pairs ? cap : 0, h_count,
+                  nullptr, 0, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int prt_join_sorted(const prt_tree *t, const void *d_queries, int coord_type, int64_t nq, prt_pair *d_pairs,
+                    int64_t cap, int64_t *h_count, void *stream) {
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  int64_t np = 0;
+  int rc = run_join(t, d_queries, coord_type, nq, reinterpret_cast<uint2 *>(d_pairs), d_pairs ? cap : 0, &np,
+                    nullptr, 0, s);
+  if (h_count) *h_count = np;
+  if (rc || np == 0) return rc;
+  PRT_CHECK(np < (1ll << 30), PRT_ERR_INVALID, "join_sorted: %lld pairs (sort limit 2^30)", (long long)np);
+  unsigned char *scr = nullptr;
+  rc = dmalloc(reinterpret_cast<void **>(&scr), 64 + np * (8 + 8 + 4 + 4), s);
+  if (rc) return rc;
+  unsigned *err = reinterpret_cast<unsigned *>(scr);
+  int *sel = reinterpret_cast<int *>(scr + 8);
+  uint64_t *k0 = reinterpret_cast<uint64_t *>(scr + 64), *k1 = k0 + np;
+  uint32_t *v0 = reinterpret_cast<uint32_t *>(k1 + np), *v1 = v0 + np;
+  cudaMemsetAsync(err, 0, 8, s);
+  int g = grid_for(np, 256, 16);
+  {
+    PRT_PROF("pair_key", s);
+    pair_key_kernel<<<g, 256, 0, s>>>(reinterpret_cast<const uint2 *>(d_pairs), np, k0, v0);
+  }
+  rc = radix_sort_pairs<uint64_t>(k0, v0, k1, v1, np, 64, sel, err, s);
+  if (!rc) {
+    PRT_PROF("pair_unkey", s);
+    pair_unkey_kernel<<<g, 256, 0, s>>>(k0, k1, sel, np, reinterpret_cast<uint2 *>(d_pairs));
+  }
+  unsigned herr = 0;
+  if (!rc) {
+    cudaError_t e = cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = cuda_status(e, "join_sorted");
+  }
+  dfree(scr, s);
+  if (!rc && (herr & kErrTimeout)) {
+    set_error("join_sorted: sort look-back timed out");
+    rc = PRT_ERR_TIMEOUT;
+  }
+  return rc;
+}
+
+int prt_query_counts(const prt_tree *t, const void *d_queries, int coord_type, int64_t nq, int td_slots,
+                     int64_t *d_counts, void *stream) {
+  PRT_CHECK(d_counts != nullptr, PRT_ERR_INVALID, "d_counts is NULL");
+  int64_t np = 0;
+  return run_join(t, d_queries, coord_type, nq, nullptr, 0, &np, reinterpret_cast<long long *>(d_counts), td_slots,
+                  reinterpret_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,817 @@
+// Overlay: clip every candidate pair with GPC semantics.
+//
+// Two schedules over the same device clipper (prt_gpc.cuh):
+//   PLAIN    one thread per pair in the order given (the reference's Execute,
+//            vector_map_overlay_gpc_kernel.cu:81-113), each with an arena
+//            slice sized for its own vertex count; launched in chunks that fit
+//            the memory budget.
+//   BATCHED  pairs sorted by vertex count (radix sort, descending) and cut
+//            into size bins; each bin is ONE persistent launch whose workers
+//            own a fixed arena slice and take the next 32 pairs per warp from
+//            an atomic ticket, so a warp's lanes clip pairs of similar cost.
+// Results go to shared pools through atomic bump reservations (contours and
+// vertices), the device analogue of the reference's per-pair device malloc
+// (GPC:703-718).  Pairs whose slice or pool reservation was too small are
+// retried with larger slices / grown pools.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "prt_gpc.cuh"
+#include "prt_internal.cuh"
+#include "prt_overlay.cuh"
+
+namespace prt {
+
+// per-pair status: ok, arena slice too small (retried), pair ids out of range,
+// result pool full (retried), malformed internal list (reported as an error)
+enum : int { kPairOk = 0, kPairArena = 1, kPairInvalid = 2, kPairPool = 3, kPairCorrupt = 4 };
+
+struct ClipOut {
+  int32_t *status;
+  int64_t *pair_cstart;
+  int32_t *pair_ncont;
+  int64_t *cont_vstart;
+  int32_t *cont_nverts;
+  int32_t *cont_hole;
+  double *xy;
+  unsigned long long *pool;  // [0] contours reserved, [1] vertices reserved
+  int64_t cap_c, cap_v;
+  double *area;  // area-only mode when non-null
+};
+
+__device__ inline bool resolve(const PairSrc &S, int64_t i, gpc::PolyView &a, gpc::PolyView &b, int64_t &nv) {
+  int64_t pa, pb;
+  if (S.pairs) {
+    uint2 p = S.pairs[i];
+    int64_t leaf = (int64_t)(int32_t)p.x - S.offset;
+    pa = S.leaf_to_poly ? (leaf >= 0 ? (int64_t)S.leaf_to_poly[leaf] : -1) : leaf;
+    pb = (int64_t)(int32_t)p.y;
+  } else {
+    pa = S.pa[i];
+    pb = S.pb[i];
+  }
+  if (pa < 0 || pa >= S.base.n_poly || pb < 0 || pb >= S.over.n_poly) return false;
+  a.ring_vert = S.base.ring_vert;
+  a.xy = S.base.xy;
+  a.r0 = S.base.poly_ring[pa];
+  a.r1 = S.base.poly_ring[pa + 1];
+  b.ring_vert = S.over.ring_vert;
+  b.xy = S.over.xy;
+  b.r0 = S.over.poly_ring[pb];
+  b.r1 = S.over.poly_ring[pb + 1];
+  nv = (a.ring_vert[a.r1] - a.ring_vert[a.r0]) + (b.ring_vert[b.r1] - b.ring_vert[b.r0]);
+  return true;
+}
+
+__device__ void process_pair(const PairSrc &S, const ClipOut &O, int64_t i, unsigned char *slice, int scale) {
+  gpc::PolyView a, b;
+  int64_t nv = 0;
+  if (!resolve(S, i, a, b, nv)) {
+    O.status[i] = kPairInvalid;
+    if (O.pair_ncont) O.pair_ncont[i] = 0;
+    if (O.area) O.area[i] = 0.0;
+    return;
+  }
+  gpc::Arena A;
+  gpc::arena_init(A, slice, gpc::caps_for(nv, scale));
+  int head = gpc::clip_pair(A, S.op, a, b);
+  int nc = 0;
+  int64_t nvt = 0;
+  if (!A.status) gpc::count_result(A, head, &nc, &nvt);
+  if (A.status) {
+    O.status[i] = A.status == gpc::kClipCapacity ? kPairArena : kPairCorrupt;
+    if (O.pair_ncont) O.pair_ncont[i] = 0;
+    return;
+  }
+  if (O.area) {
+    O.area[i] = nc ? gpc::result_area(A, head) : 0.0;
+    O.status[i] = kPairOk;
+    return;
+  }
+  int64_t cbase = 0, vbase = 0;
+  if (nc) {
+    cbase = (int64_t)atomicAdd(&O.pool[0], (unsigned long long)nc);
+    vbase = (int64_t)atomicAdd(&O.pool[1], (unsigned long long)nvt);
+    if (cbase + nc > O.cap_c || vbase + nvt > O.cap_v) {
+      O.status[i] = kPairPool;
+      return;
+    }
+    gpc::write_result(A, head, O.cont_nverts, O.cont_hole, O.cont_vstart, O.xy, cbase, vbase);
+  }
+  O.pair_cstart[i] = cbase;
+  O.pair_ncont[i] = nc;
+  O.status[i] = kPairOk;
+}
+
+namespace {
+
+__global__ void nv_kernel(PairSrc S, int64_t n, const int64_t *__restrict__ idx, int scale, int64_t *__restrict__ nv,
+                          int64_t *__restrict__ demand) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i = idx ? idx[t] : t;
+    gpc::PolyView a, b;
+    int64_t v = 0;
+    if (!resolve(S, i, a, b, v)) v = 0;
+    if (nv) nv[t] = v;
+    if (demand) demand[t] = (int64_t)gpc::arena_bytes(gpc::caps_for(v, scale));
+  }
+}
+
+__global__ void __launch_bounds__(128) clip_plain_kernel(PairSrc S, ClipOut O, const int64_t *__restrict__ idx,
+                                                         int64_t begin, int64_t count, unsigned char *arena,
+                                                         const int64_t *__restrict__ arena_off, int64_t off_base,
+                                                         int scale) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  int64_t k = begin + t;
+  int64_t i = idx ? idx[k] : k;
+  process_pair(S, O, i, arena + (arena_off[k] - off_base), scale);
+}
+
+__global__ void __launch_bounds__(128) clip_batched_kernel(PairSrc S, ClipOut O, const uint32_t *__restrict__ order,
+                                                           int64_t begin, int64_t end,
+                                                           unsigned long long *ticket, unsigned char *arena,
+                                                           size_t slice_bytes, int64_t workers, int scale) {
+  const int lane = threadIdx.x & 31;
+  const int64_t worker = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (worker >= workers) return;  // workers is a multiple of 32: whole warps leave
+  unsigned char *slice = arena + worker * slice_bytes;
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(ticket, 32ull);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    int64_t k = begin + (int64_t)base + lane;
+    if (begin + (int64_t)base >= end) break;
+    if (k < end) process_pair(S, O, (int64_t)order[k], slice, scale);
+  }
+}
+
+// Sort keys: larger vertex counts first.
+__global__ void size_key_kernel(const int64_t *__restrict__ nv, int64_t n, uint32_t *__restrict__ key,
+                                uint32_t *__restrict__ val) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t v = nv[i];
+    key[i] = 0xFFFFFFFFu - (uint32_t)(v > 0xFFFFFFFFll ? 0xFFFFFFFFll : v);
+    val[i] = (uint32_t)i;
+  }
+}
+
+// bounds[b] = first sorted position whose vertex count is <= thr[b]
+// (counts descend along the sorted order); maxnv[b] = count at that position.
+__global__ void bin_bounds_kernel(const uint32_t *__restrict__ k0, const uint32_t *__restrict__ k1,
+                                  const int *__restrict__ sel, int64_t n, const int64_t *__restrict__ thr, int nbins,
+                                  int64_t *__restrict__ bounds, int64_t *__restrict__ maxnv) {
+  const uint32_t *k = *sel ? k1 : k0;
+  int b = threadIdx.x;
+  if (b >= nbins) return;
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t mid = (lo + hi) / 2;
+    int64_t v = (int64_t)(0xFFFFFFFFu - k[mid]);
+    if (v > thr[b]) lo = mid + 1;
+    else hi = mid;
+  }
+  bounds[b] = lo;
+  maxnv[b] = lo < n ? (int64_t)(0xFFFFFFFFu - k[lo]) : 0;
+}
+
+__global__ void select_u32_kernel(const uint32_t *a, const uint32_t *b, const int *sel, int64_t n, uint32_t *dst) {
+  const uint32_t *src = *sel ? b : a;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+__global__ void area_from_results_kernel(const int64_t *__restrict__ pair_cstart, const int32_t *__restrict__ pair_ncont,
+                                         const int64_t *__restrict__ cont_vstart, const int32_t *__restrict__ cont_nverts,
+                                         const int32_t *__restrict__ cont_hole, const double *__restrict__ xy, int64_t n,
+                                         double *__restrict__ area) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double total = 0.0;
+    for (int c = 0; c < pair_ncont[i]; c++) {
+      int64_t cc = pair_cstart[i] + c;
+      const double *v = xy + 2 * cont_vstart[cc];
+      int m = cont_nverts[cc];
+      double a = 0.0;
+      for (int j = 0; j < m; j++) {
+        int k = (j + 1) % m;
+        a += v[2 * j] * v[2 * k + 1] - v[2 * k] * v[2 * j + 1];
+      }
+      a = 0.5 * fabs(a);
+      total += cont_hole[cc] ? -a : a;
+    }
+    area[i] = total;
+  }
+}
+
+size_t arena_budget() {
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    cudaGetLastError();
+    return (size_t)1 << 30;
+  }
+  size_t b = fr / 3;
+  const size_t cap = (size_t)48 << 30;
+  return std::max<size_t>(std::min(b, cap), (size_t)64 << 20);
+}
+
+}  // namespace
+
+// Bins for the batched schedule: upper bounds on the pair vertex count.
+static const int64_t kBinThresholds[] = {1ll << 40, 4096, 1024, 256, 64};
+static const int kNumBins = 5;
+
+struct OverlayState {
+  PairSrc S;
+  ClipOut O;
+  int64_t n;
+  int64_t retried = 0;
+};
+
+static int grow_pools(OverlayState &st, cudaStream_t s, int64_t need_c, int64_t need_v) {
+  unsigned long long used[2];
+  PRT_CUDA(cudaMemcpyAsync(used, st.O.pool, sizeof used, cudaMemcpyDeviceToHost, s));
+  PRT_CUDA(cudaStreamSynchronize(s));
+  int64_t nc = std::max<int64_t>(2 * st.O.cap_c, (int64_t)used[0] + need_c + 1024);
+  int64_t nvv = std::max<int64_t>(2 * st.O.cap_v, (int64_t)used[1] + need_v + 1024);
+  int64_t *cvs = nullptr;
+  int32_t *cnv = nullptr, *ch = nullptr;
+  double *xy = nullptr;
+  int rc = dalloc(&cvs, nc, s);
+  if (!rc) rc = dalloc(&cnv, nc, s);
+  if (!rc) rc = dalloc(&ch, nc, s);
+  if (!rc) rc = dalloc(&xy, 2 * nvv, s);
+  if (rc) {
+    dfree(cvs, s);
+    dfree(cnv, s);
+    dfree(ch, s);
+    return rc;
+  }
+  int64_t kc = std::min<int64_t>((int64_t)used[0], st.O.cap_c), kv = std::min<int64_t>((int64_t)used[1], st.O.cap_v);
+  if (kc) {
+    cudaMemcpyAsync(cvs, st.O.cont_vstart, 8 * kc, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(cnv, st.O.cont_nverts, 4 * kc, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(ch, st.O.cont_hole, 4 * kc, cudaMemcpyDeviceToDevice, s);
+  }
+  if (kv) cudaMemcpyAsync(xy, st.O.xy, 16 * kv, cudaMemcpyDeviceToDevice, s);
+  dfree(st.O.cont_vstart, s);
+  dfree(st.O.cont_nverts, s);
+  dfree(st.O.cont_hole, s);
+  dfree(st.O.xy, s);
+  st.O.cont_vstart = cvs;
+  st.O.cont_nverts = cnv;
+  st.O.cont_hole = ch;
+  st.O.xy = xy;
+  st.O.cap_c = nc;
+  st.O.cap_v = nvv;
+  PRT_CUDA(cudaGetLastError());
+  return PRT_OK;
+}
+
+// Plain launches over items [0, count) of idx (or all pairs when idx is
+// NULL), chunked by the arena budget.
+static int run_plain(OverlayState &st, const int64_t *d_idx, int64_t count, int scale, cudaStream_t s) {
+  if (count == 0) return PRT_OK;
+  int64_t *demand = nullptr, *off = nullptr;
+  int rc = dalloc(&demand, count, s);
+  if (!rc) rc = dalloc(&off, count + 1, s);
+  if (rc) {
+    dfree(demand, s);
+    return rc;
+  }
+  {
+    PRT_PROF("nv", s);
+    nv_kernel<<<grid_for(count, 256, 16), 256, 0, s>>>(st.S, count, d_idx, scale, nullptr, demand);
+  }
+  rc = exclusive_scan<int64_t>(demand, count, off, off + count, s);
+  std::vector<int64_t> h_off(count + 1);
+  if (!rc) {
+    cudaError_t e = cudaMemcpyAsync(h_off.data(), off, 8 * (count + 1), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = cuda_status(e, "overlay plain");
+  }
+  const int64_t budget = (int64_t)arena_budget();
+  unsigned char *arena = nullptr;
+  int64_t arena_cap = 0;
+  int64_t b = 0;
+  while (!rc && b < count) {
+    int64_t e = b + 1;
+    // largest chunk [b, e) that fits the budget (at least one pair)
+    int64_t lo = b + 1, hi = count;
+    while (lo < hi) {
+      int64_t mid = (lo + hi + 1) / 2;
+      if (h_off[mid] - h_off[b] <= budget) lo = mid;
+      else hi = mid - 1;
+    }
+    e = lo;
+    int64_t bytes = h_off[e] - h_off[b];
+    if (bytes > arena_cap) {
+      dfree(arena, s);
+      arena = nullptr;
+      rc = dmalloc(reinterpret_cast<void **>(&arena), bytes, s);
+      if (rc) break;
+      arena_cap = bytes;
+    }
+    int64_t cnt = e - b;
+    {
+      PRT_PROF("clip_plain", s);
+      clip_plain_kernel<<<(unsigned)((cnt + 127) / 128), 128, 0, s>>>(st.S, st.O, d_idx, b, cnt, arena, off, h_off[b],
+                                                                    scale);
+    }
+    b = e;
+  }
+  if (!rc) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) rc = cuda_status(e, "clip_plain_kernel");
+  }
+  dfree(arena, s);
+  dfree(demand, s);
+  dfree(off, s);
+  return rc;
+}
+
+static int run_batched(OverlayState &st, cudaStream_t s) {
+  const int64_t n = st.n;
+  int64_t *nv = nullptr;
+  unsigned char *scr = nullptr;
+  int rc = dalloc(&nv, n, s);
+  if (!rc) rc = dmalloc(reinterpret_cast<void **>(&scr), 256 + 16 * n + 4 * n, s);
+  if (rc) {
+    dfree(nv, s);
+    return rc;
+  }
+  unsigned *err = reinterpret_cast<unsigned *>(scr);
+  int *sel = reinterpret_cast<int *>(scr + 8);
+  int64_t *thr = reinterpret_cast<int64_t *>(scr + 16);   // kNumBins
+  int64_t *bnd = thr + 8;                                 // kNumBins
+  int64_t *mx = bnd + 8;                                  // kNumBins
+  unsigned long long *tickets = reinterpret_cast<unsigned long long *>(mx + 8);  // kNumBins
+  uint32_t *k0 = reinterpret_cast<uint32_t *>(scr + 256);
+  uint32_t *k1 = k0 + n, *v0 = k1 + n, *v1 = v0 + n, *order = v1 + n;
+  cudaMemsetAsync(scr, 0, 256, s);
+  cudaMemcpyAsync(thr, kBinThresholds, sizeof(int64_t) * kNumBins, cudaMemcpyHostToDevice, s);
+  const int g = grid_for(n, 256, 16);
+  {
+    PRT_PROF("nv", s);
+    nv_kernel<<<g, 256, 0, s>>>(st.S, n, nullptr, 1, nv, nullptr);
+  }
+  {
+    PRT_PROF("size_key", s);
+    size_key_kernel<<<g, 256, 0, s>>>(nv, n, k0, v0);
+  }
+  rc = radix_sort_pairs<uint32_t>(k0, v0, k1, v1, n, 32, sel, err, s);
+  int64_t hb[8] = {0}, hm[8] = {0};
+  if (!rc) {
+    {
+      PRT_PROF("select_u32", s);
+      select_u32_kernel<<<g, 256, 0, s>>>(v0, v1, sel, n, order);
+    }
+    {
+      PRT_PROF("bin_bounds", s);
+      bin_bounds_kernel<<<1, 32, 0, s>>>(k0, k1, sel, n, thr, kNumBins, bnd, mx);
+    }
+    cudaMemcpyAsync(hb, bnd, sizeof(int64_t) * kNumBins, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hm, mx, sizeof(int64_t) * kNumBins, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = cuda_status(e, "overlay batched");
+  }
+  // bin b covers sorted positions [bnd[b], bnd[b+1]) (bnd[kNumBins] = n)
+  hb[kNumBins] = n;
+  const size_t budget = arena_budget();
+  const int64_t resident = (int64_t)kSMs * 1024;
+  unsigned char *arena = nullptr;
+  size_t arena_cap = 0;
+  for (int bi = 0; bi < kNumBins && !rc; bi++) {
+    int64_t b0 = hb[bi], b1 = hb[bi + 1];
+    if (b1 <= b0) continue;
+    const int64_t maxnv = hm[bi];
+    const size_t slice = gpc::arena_bytes(gpc::caps_for(maxnv, 1));
+    int64_t workers = std::min<int64_t>(b1 - b0, resident);
+    workers = std::min<int64_t>(workers, (int64_t)(budget / slice));
+    workers = std::max<int64_t>(32, (workers + 31) / 32 * 32);
+    size_t need = slice * (size_t)workers;
+    if (need > arena_cap) {
+      dfree(arena, s);
+      arena = nullptr;
+      rc = dmalloc(reinterpret_cast<void **>(&arena), need, s);
+      if (rc) break;
+      arena_cap = need;
+    }
+    {
+      PRT_PROF("clip_batched", s);
+      clip_batched_kernel<<<(unsigned)((workers + 127) / 128), 128, 0, s>>>(st.S, st.O, order, b0, b1, &tickets[bi],
+                                                                          arena, slice, workers, 1);
+    }
+  }
+  if (!rc) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) rc = cuda_status(e, "clip_batched_kernel");
+  }
+  dfree(arena, s);
+  dfree(nv, s);
+  dfree(scr, s);
+  return rc;
+}
+
+// Retries pairs whose arena slice or pool reservation was too small.
+static int retry_failed(OverlayState &st, cudaStream_t s) {
+  const int64_t n = st.n;
+  std::vector<int32_t> hs(n);
+  for (int round = 0; round < 6; round++) {
+    PRT_CUDA(cudaMemcpyAsync(hs.data(), st.O.status, 4 * n, cudaMemcpyDeviceToHost, s));
+    PRT_CUDA(cudaStreamSynchronize(s));
+    std::vector<int64_t> fail;
+    bool pool = false;
+    for (int64_t i = 0; i < n; i++) {
+      if (hs[i] == kPairArena || hs[i] == kPairPool) {
+        fail.push_back(i);
+        pool |= hs[i] == kPairPool;
+      } else if (hs[i] == kPairInvalid) {
+        set_error("overlay: pair %lld names a polygon outside its layer", (long long)i);
+        return PRT_ERR_INVALID;
+      } else if (hs[i] == kPairCorrupt) {
+        set_error("overlay: pair %lld: clipper list walk exceeded its bound", (long long)i);
+        return PRT_ERR_INVALID;
+      }
+    }
+    if (fail.empty()) return PRT_OK;
+    st.retried += (int64_t)fail.size();
+    if (pool) {
+      int rc = grow_pools(st, s, 0, 0);
+      if (rc) return rc;
+    }
+    int64_t *d_idx = nullptr;
+    int rc = dalloc(&d_idx, fail.size(), s);
+    if (rc) return rc;
+    cudaMemcpyAsync(d_idx, fail.data(), 8 * fail.size(), cudaMemcpyHostToDevice, s);
+    rc = run_plain(st, d_idx, (int64_t)fail.size(), 1 << (2 * (round + 1)), s);
+    dfree(d_idx, s);
+    if (rc) return rc;
+  }
+  set_error("overlay: pairs still exceed the largest arena after retries");
+  return PRT_ERR_CAPACITY;
+}
+
+}  // namespace prt
+
+struct prt_results {
+  int64_t n_pairs, n_cont, n_vert, nonempty, retried;
+  int64_t *pair_cstart;
+  int32_t *pair_ncont;
+  int32_t *status;
+  int64_t *cont_vstart;
+  int32_t *cont_nverts;
+  int32_t *cont_hole;
+  double *xy;
+  unsigned long long *pool;
+};
+
+namespace prt {
+
+static void free_state(OverlayState &st, cudaStream_t s) {
+  dfree(st.O.status, s);
+  dfree(st.O.pair_cstart, s);
+  dfree(st.O.pair_ncont, s);
+  dfree(st.O.cont_vstart, s);
+  dfree(st.O.cont_nverts, s);
+  dfree(st.O.cont_hole, s);
+  dfree(st.O.xy, s);
+  dfree(st.O.pool, s);
+}
+
+// area != nullptr: area-only mode (no contour output, no results object).
+int overlay_impl(const PairSrc &S, int64_t n, int sched, double *d_area, cudaStream_t s, prt_results **out) {
+  PRT_CHECK(n >= 0 && n < (1ll << 31), PRT_ERR_INVALID, "n_pairs=%lld", (long long)n);
+  PRT_CHECK(S.op >= 0 && S.op <= 3, PRT_ERR_INVALID, "op %d", S.op);
+  PRT_CHECK(sched == PRT_SCHED_PLAIN || sched == PRT_SCHED_BATCHED, PRT_ERR_INVALID, "sched %d", sched);
+  OverlayState st;
+  st.S = S;
+  st.n = n;
+  memset(&st.O, 0, sizeof st.O);
+  st.O.area = d_area;
+  int rc = dalloc(&st.O.status, std::max<int64_t>(n, 1), s);
+  if (!rc) rc = dalloc(&st.O.pool, 2, s);
+  if (!rc && !d_area) rc = dalloc(&st.O.pair_cstart, std::max<int64_t>(n, 1), s);
+  if (!rc && !d_area) rc = dalloc(&st.O.pair_ncont, std::max<int64_t>(n, 1), s);
+  int64_t total_nv = 0;
+  if (!rc && !d_area && n > 0) {
+    int64_t *nv = nullptr, *tmp = nullptr;
+    rc = dalloc(&nv, n, s);
+    if (!rc) rc = dalloc(&tmp, n + 1, s);
+    if (!rc) {
+      {
+        PRT_PROF("nv", s);
+        nv_kernel<<<grid_for(n, 256, 16), 256, 0, s>>>(S, n, nullptr, 1, nv, nullptr);
+      }
+      rc = exclusive_scan<int64_t>(nv, n, tmp, tmp + n, s);
+    }
+    if (!rc) {
+      cudaError_t e = cudaMemcpyAsync(&total_nv, tmp + n, 8, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) rc = cuda_status(e, "overlay sizes");
+    }
+    dfree(nv, s);
+    dfree(tmp, s);
+  }
+  if (!rc && !d_area) {
+    st.O.cap_c = total_nv / 4 + 1024;
+    st.O.cap_v = total_nv + 4096;
+    rc = dalloc(&st.O.cont_vstart, st.O.cap_c, s);
+    if (!rc) rc = dalloc(&st.O.cont_nverts, st.O.cap_c, s);
+    if (!rc) rc = dalloc(&st.O.cont_hole, st.O.cap_c, s);
+    if (!rc) rc = dalloc(&st.O.xy, 2 * st.O.cap_v, s);
+  }
+  if (!rc) {
+    cudaError_t e = cudaMemsetAsync(st.O.pool, 0, 16, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(st.O.status, 0, 4 * std::max<int64_t>(n, 1), s);
+    if (e != cudaSuccess) rc = cuda_status(e, "memset");
+  }
+  if (!rc && n > 0) rc = sched == PRT_SCHED_PLAIN ? run_plain(st, nullptr, n, 1, s) : run_batched(st, s);
+  if (!rc && n > 0) rc = retry_failed(st, s);
+  if (rc || d_area) {
+    if (!rc) {
+      cudaError_t e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) rc = cuda_status(e, "overlay");
+    }
+    free_state(st, s);
+    return rc;
+  }
+  prt_results *r = new prt_results();
+  r->n_pairs = n;
+  r->retried = st.retried;
+  r->pair_cstart = st.O.pair_cstart;
+  r->pair_ncont = st.O.pair_ncont;
+  r->status = st.O.status;
+  r->cont_vstart = st.O.cont_vstart;
+  r->cont_nverts = st.O.cont_nverts;
+  r->cont_hole = st.O.cont_hole;
+  r->xy = st.O.xy;
+  r->pool = st.O.pool;
+  // exact totals from the per-pair counts
+  {
+    std::vector<int32_t> nc(n);
+    cudaError_t e = cudaMemcpyAsync(nc.data(), r->pair_ncont, 4 * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      prt_results_free(r);
+      return cuda_status(e, "overlay results");
+    }
+    int64_t c = 0, ne = 0;
+    for (int64_t i = 0; i < n; i++) {
+      c += nc[i];
+      ne += nc[i] > 0;
+    }
+    r->n_cont = c;
+    r->nonempty = ne;
+    unsigned long long used[2];
+    cudaMemcpy(used, r->pool, sizeof used, cudaMemcpyDeviceToHost);
+    r->n_vert = (int64_t)used[1];
+  }
+  *out = r;
+  return PRT_OK;
+}
+
+__global__ void ident_rings_kernel(int64_t n, int64_t *poly_ring) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x)
+    poly_ring[i] = i;
+}
+
+__global__ void ring_vert_from_ref_kernel(const int32_t *num, const int64_t *prefix, int64_t n, int64_t *ring_vert) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    ring_vert[i] = prefix[i];
+    if (i == n - 1) ring_vert[n] = prefix[i] + num[i];
+  }
+}
+
+}  // namespace prt
+
+using namespace prt;
+
+extern "C" {
+
+int prt_overlay_run(const prt_pair *d_pairs, int64_t n_pairs, int32_t offset, const int32_t *d_leaf_to_poly,
+                    const prt_layer *base, const prt_layer *overlay, int op, int sched, void *stream,
+                    prt_results **out) {
+  PRT_CHECK(out && base && overlay, PRT_ERR_INVALID, "NULL argument");
+  PRT_CHECK(d_pairs || n_pairs == 0, PRT_ERR_INVALID, "d_pairs is NULL");
+  *out = nullptr;
+  PairSrc S;
+  memset(&S, 0, sizeof S);
+  S.pairs = reinterpret_cast<const uint2 *>(d_pairs);
+  S.offset = offset;
+  S.leaf_to_poly = d_leaf_to_poly;
+  S.base = layer_dev(base);
+  S.over = layer_dev(overlay);
+  S.op = op;
+  return overlay_impl(S, n_pairs, sched, nullptr, reinterpret_cast<cudaStream_t>(stream), out);
+}
+
+// The reference's per-polygon CSR (readData packs polygon i's vertices at
+// [prefix[i], prefix[i] + num[i]) with prefix[i+1] = prefix[i] + num[i]) is a
+// ring CSR with one ring per polygon: poly_ring = 0..n, ring_vert = prefix
+// followed by the total.  The packing is checked before use.
+static int ref_layer(const int32_t *num, const int64_t *prefix, int64_t n, int64_t **pr, int64_t **rv,
+                     cudaStream_t s) {
+  std::vector<int32_t> hn(n);
+  std::vector<int64_t> hp(n);
+  PRT_CUDA(cudaMemcpyAsync(hn.data(), num, 4 * n, cudaMemcpyDeviceToHost, s));
+  PRT_CUDA(cudaMemcpyAsync(hp.data(), prefix, 8 * n, cudaMemcpyDeviceToHost, s));
+  PRT_CUDA(cudaStreamSynchronize(s));
+  for (int64_t i = 0; i + 1 < n; i++)
+    PRT_CHECK(hp[i + 1] == hp[i] + hn[i], PRT_ERR_INVALID, "prefix[%lld] is not prefix[%lld] + num[%lld]",
+              (long long)(i + 1), (long long)i, (long long)i);
+  int rc = dalloc(pr, n + 1, s);
+  if (!rc) rc = dalloc(rv, n + 1, s);
+  if (rc) return rc;
+  {
+    PRT_PROF("ident_rings", s);
+    ident_rings_kernel<<<grid_for(n + 1, 256, 4), 256, 0, s>>>(n, *pr);
+  }
+  {
+    PRT_PROF("ring_vert_from_ref", s);
+    ring_vert_from_ref_kernel<<<grid_for(n, 256, 4), 256, 0, s>>>(num, prefix, n, *rv);
+  }
+  PRT_CUDA(cudaGetLastError());
+  return PRT_OK;
+}
+
+int prt_overlay_run_ref(const prt_pair *d_pairs, int64_t n_pairs, int32_t offset, const int32_t *d_leaf_to_poly,
+                        const int32_t *d_num_base, const int64_t *d_prefix_base, const double *d_vertex_base,
+                        const int32_t *d_hole_base, int64_t n_base, const int32_t *d_num_overlay,
+                        const int64_t *d_prefix_overlay, const double *d_vertex_overlay,
+                        const int32_t *d_hole_overlay, int64_t n_overlay, int op, int sched, void *stream,
+                        prt_results **out) {
+  PRT_CHECK(out, PRT_ERR_INVALID, "out is NULL");
+  PRT_CHECK(n_base > 0 && n_overlay > 0, PRT_ERR_INVALID, "empty layer");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  // the hole flags are carried by the reference but not read by its clip
+  (void)d_hole_base;
+  (void)d_hole_overlay;
+  int64_t *pr_b = nullptr, *rv_b = nullptr, *pr_o = nullptr, *rv_o = nullptr;
+  int rc = ref_layer(d_num_base, d_prefix_base, n_base, &pr_b, &rv_b, s);
+  if (!rc) rc = ref_layer(d_num_overlay, d_prefix_overlay, n_overlay, &pr_o, &rv_o, s);
+  if (!rc) {
+    PairSrc S;
+    memset(&S, 0, sizeof S);
+    S.pairs = reinterpret_cast<const uint2 *>(d_pairs);
+    S.offset = offset;
+    S.leaf_to_poly = d_leaf_to_poly;
+    S.op = op;
+    S.base.poly_ring = pr_b;
+    S.base.ring_vert = rv_b;
+    S.base.xy = d_vertex_base;
+    S.base.n_poly = n_base;
+    S.over.poly_ring = pr_o;
+    S.over.ring_vert = rv_o;
+    S.over.xy = d_vertex_overlay;
+    S.over.n_poly = n_overlay;
+    rc = overlay_impl(S, n_pairs, sched, nullptr, s, out);
+  }
+  cudaStreamSynchronize(s);
+  dfree(pr_b, s);
+  dfree(rv_b, s);
+  dfree(pr_o, s);
+  dfree(rv_o, s);
+  return rc;
+}
+
+int prt_results_sizes(const prt_results *r, int64_t *sizes) {
+  PRT_CHECK(r && sizes, PRT_ERR_INVALID, "NULL argument");
+  sizes[0] = r->n_pairs;
+  sizes[1] = r->n_cont;
+  sizes[2] = r->n_vert;
+  sizes[3] = r->nonempty;
+  sizes[4] = r->retried;
+  return PRT_OK;
+}
+
+int prt_results_device(const prt_results *r, const int64_t **pair_cont_start, const int32_t **pair_ncont,
+                       const int64_t **cont_vert_start, const int32_t **cont_nverts, const int32_t **cont_hole,
+                       const double **xy) {
+  PRT_CHECK(r, PRT_ERR_INVALID, "NULL argument");
+  if (pair_cont_start) *pair_cont_start = r->pair_cstart;
+  if (pair_ncont) *pair_ncont = r->pair_ncont;
+  if (cont_vert_start) *cont_vert_start = r->cont_vstart;
+  if (cont_nverts) *cont_nverts = r->cont_nverts;
+  if (cont_hole) *cont_hole = r->cont_hole;
+  if (xy) *xy = r->xy;
+  return PRT_OK;
+}
+
+int prt_results_copy(const prt_results *r, int64_t *h_pair_cont_off, int32_t *h_cont_nverts, int32_t *h_cont_hole,
+                     double *h_xy) {
+  PRT_CHECK(r && h_pair_cont_off && h_cont_nverts && h_cont_hole && h_xy, PRT_ERR_INVALID, "NULL argument");
+  const int64_t n = r->n_pairs;
+  unsigned long long used[2];
+  PRT_CUDA(cudaDeviceSynchronize());
+  PRT_CUDA(cudaMemcpy(used, r->pool, sizeof used, cudaMemcpyDeviceToHost));
+  std::vector<int64_t> cs(n), cvs(used[0]);
+  std::vector<int32_t> nc(n), cnv(used[0]), ch(used[0]);
+  std::vector<double> xy(2 * used[1]);
+  PRT_CUDA(cudaMemcpy(cs.data(), r->pair_cstart, 8 * n, cudaMemcpyDeviceToHost));
+  PRT_CUDA(cudaMemcpy(nc.data(), r->pair_ncont, 4 * n, cudaMemcpyDeviceToHost));
+  if (used[0]) {
+    PRT_CUDA(cudaMemcpy(cvs.data(), r->cont_vstart, 8 * used[0], cudaMemcpyDeviceToHost));
+    PRT_CUDA(cudaMemcpy(cnv.data(), r->cont_nverts, 4 * used[0], cudaMemcpyDeviceToHost));
+    PRT_CUDA(cudaMemcpy(ch.data(), r->cont_hole, 4 * used[0], cudaMemcpyDeviceToHost));
+  }
+  if (used[1]) PRT_CUDA(cudaMemcpy(xy.data(), r->xy, 16 * used[1], cudaMemcpyDeviceToHost));
+  int64_t c = 0, v = 0;
+  h_pair_cont_off[0] = 0;
+  for (int64_t i = 0; i < n; i++) {
+    for (int k = 0; k < nc[i]; k++) {
+      int64_t cc = cs[i] + k;
+      h_cont_nverts[c] = cnv[cc];
+      h_cont_hole[c] = ch[cc];
+      memcpy(h_xy + 2 * v, xy.data() + 2 * cvs[cc], 16 * (size_t)cnv[cc]);
+      v += cnv[cc];
+      c++;
+    }
+    h_pair_cont_off[i + 1] = c;
+  }
+  return PRT_OK;
+}
+
+int prt_results_area(const prt_results *r, double *d_area, void *stream) {
+  PRT_CHECK(r && d_area, PRT_ERR_INVALID, "NULL argument");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (r->n_pairs == 0) return PRT_OK;
+  {
+    PRT_PROF("area_from_results", s);
+    area_from_results_kernel<<<grid_for(r->n_pairs, 256, 16), 256, 0, s>>>(
+      r->pair_cstart, r->pair_ncont, r->cont_vstart, r->cont_nverts, r->cont_hole, r->xy, r->n_pairs, d_area);
+  }
+  PRT_CUDA(cudaGetLastError());
+  return PRT_OK;
+}
+
+int prt_results_free(prt_results *r) {
+  if (!r) return PRT_OK;
+  cudaFree(r->pair_cstart);
+  cudaFree(r->pair_ncont);
+  cudaFree(r->status);
+  cudaFree(r->cont_vstart);
+  cudaFree(r->cont_nverts);
+  cudaFree(r->cont_hole);
+  cudaFree(r->xy);
+  cudaFree(r->pool);
+  delete r;
+  return PRT_OK;
+}
+
+int prt_clip_pair_host(int op, int s_ncont, const int32_t *s_nverts, const double *s_xy, int c_ncont,
+                       const int32_t *c_nverts, const double *c_xy, int32_t *out_ncont, int32_t cont_cap,
+                       int32_t *out_nverts, int32_t *out_hole, int64_t *out_nv, int64_t vert_cap, double *out_xy) {
+  PRT_CHECK(out_ncont && out_nv && (s_ncont == 0 || (s_nverts && s_xy)) && (c_ncont == 0 || (c_nverts && c_xy)),
+            PRT_ERR_INVALID, "NULL argument");
+  PRT_CHECK(s_ncont >= 0 && c_ncont >= 0, PRT_ERR_INVALID, "negative contour count");
+  cudaStream_t s = 0;
+  // layers with one polygon each (zero-ring polygons allowed)
+  std::vector<int64_t> pr_s = {0, s_ncont}, pr_c = {0, c_ncont};
+  std::vector<int64_t> rv_s(s_ncont + 1, 0), rv_c(c_ncont + 1, 0);
+  for (int i = 0; i < s_ncont; i++) rv_s[i + 1] = rv_s[i] + s_nverts[i];
+  for (int i = 0; i < c_ncont; i++) rv_c[i + 1] = rv_c[i] + c_nverts[i];
+  int64_t vs = rv_s[s_ncont], vc = rv_c[c_ncont];
+  int64_t *d_i64 = nullptr;
+  double *d_xy = nullptr;
+  int32_t *d_pair = nullptr;
+  size_t ni = 4 + (s_ncont + 1) + (c_ncont + 1);
+  PRT_CUDA(cudaMalloc(&d_i64, 8 * ni));
+  PRT_CUDA(cudaMalloc(&d_xy, 16 * (vs + vc + 1)));
+  PRT_CUDA(cudaMalloc(&d_pair, 8));
+  int64_t *d_prs = d_i64, *d_prc = d_i64 + 2, *d_rvs = d_i64 + 4, *d_rvc = d_rvs + s_ncont + 1;
+  cudaMemcpy(d_prs, pr_s.data(), 16, cudaMemcpyHostToDevice);
+  cudaMemcpy(d_prc, pr_c.data(), 16, cudaMemcpyHostToDevice);
+  cudaMemcpy(d_rvs, rv_s.data(), 8 * (s_ncont + 1), cudaMemcpyHostToDevice);
+  cudaMemcpy(d_rvc, rv_c.data(), 8 * (c_ncont + 1), cudaMemcpyHostToDevice);
+  if (vs) cudaMemcpy(d_xy, s_xy, 16 * vs, cudaMemcpyHostToDevice);
+  if (vc) cudaMemcpy(d_xy + 2 * vs, c_xy, 16 * vc, cudaMemcpyHostToDevice);
+  int32_t zero[2] = {0, 0};
+  cudaMemcpy(d_pair, zero, 8, cudaMemcpyHostToDevice);
+  prt_layer Ls = {d_prs, d_rvs, nullptr, d_xy, 1};
+  prt_layer Lc = {d_prc, d_rvc, nullptr, d_xy + 2 * vs, 1};
+  prt_results *r = nullptr;
+  int rc = prt_overlay_run(reinterpret_cast<const prt_pair *>(d_pair), 1, 0, nullptr, &Ls, &Lc, op,
+                           PRT_SCHED_PLAIN, nullptr, &r);
+  if (!rc) {
+    *out_ncont = (int32_t)r->n_cont;
+    *out_nv = r->n_vert;
+    if (r->n_cont > cont_cap || r->n_vert > vert_cap) {
+      set_error("clip_pair_host: result has %lld contours / %lld vertices", (long long)r->n_cont,
+                (long long)r->n_vert);
+      rc = PRT_ERR_CAPACITY;
+    } else if (r->n_cont > 0) {
+      std::vector<int64_t> off(2);
+      rc = prt_results_copy(r, off.data(), out_nverts, out_hole, out_xy);
+    }
+  }
+  prt_results_free(r);
+  cudaFree(d_i64);
+  cudaFree(d_xy);
+  cudaFree(d_pair);
+  (void)s;
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,289 @@
+// Onesweep LSD radix sort of (key, uint32 value) pairs.
+//
+// One upsweep kernel histograms every 8-bit digit of every key at once; a
+// tiny plan kernel scans the histograms and marks passes whose digit is the
+// same for all keys (they are skipped without a host round trip, so the whole
+// sort can be captured in a CUDA graph).  Each remaining pass is ONE kernel:
+// a CTA takes the next tile in launch order (atomic ticket), ranks its keys
+// with warp-level __match_any_sync multisplit, learns its global digit
+// offsets by decoupled look-back over the preceding tiles (bounded spin, an
+// error flag instead of a hang), stages the tile in shared memory in digit
+// order and writes it out in coalesced runs.  Stable: ranks follow the
+// original order within a warp, then warp order, then tile order.
+#include <cuda_runtime.h>
+
+#include "prt_internal.cuh"
+
+namespace prt {
+namespace {
+
+constexpr int kRadix = 256;
+constexpr int kSortBlock = 256;
+constexpr int kSortWarps = kSortBlock / 32;
+constexpr int kItems = 16;
+constexpr int kTile = kSortBlock * kItems;
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagPrefix = 2u << 30;
+constexpr uint32_t kCountMask = (1u << 30) - 1;
+
+struct PassPlan {
+  int active, src, dst, pad;
+};
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <typename KeyT>
+__global__ void __launch_bounds__(256) hist_kernel(const KeyT *__restrict__ keys, int64_t n, int passes,
+                                                   uint32_t *__restrict__ ghist) {
+  extern __shared__ uint32_t sh[];  // passes * 256
+  for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    KeyT k = keys[i];
+    for (int p = 0; p < passes; p++) atomicAdd(&sh[p * kRadix + (int)((k >> (8 * p)) & 0xFF)], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x)
+    if (sh[i]) atomicAdd(&ghist[i], sh[i]);
+}
+
+__global__ void plan_kernel(const uint32_t *__restrict__ ghist, uint32_t *__restrict__ goff, int passes, int64_t n,
+                            PassPlan *__restrict__ plan, int *__restrict__ d_sel) {
+  __shared__ uint32_t scan[kRadix];
+  __shared__ int trivial[PRT_MAX_LEVELS];
+  for (int p = 0; p < passes; p++) {
+    uint32_t c = ghist[p * kRadix + threadIdx.x];
+    scan[threadIdx.x] = c;
+    if (threadIdx.x == 0) trivial[p] = 0;
+    __syncthreads();
+    if ((int64_t)c == n) trivial[p] = 1;
+    // inclusive Hillis-Steele scan over 256 bins
+    for (int o = 1; o < kRadix; o <<= 1) {
+      uint32_t v = threadIdx.x >= o ? scan[threadIdx.x - o] : 0u;
+      __syncthreads();
+      scan[threadIdx.x] += v;
+      __syncthreads();
+    }
+    goff[p * kRadix + threadIdx.x] = scan[threadIdx.x] - c;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    int cur = 0;
+    for (int p = 0; p < passes; p++) {
+      PassPlan pp;
+      pp.active = !trivial[p];
+      pp.src = cur;
+      pp.dst = 1 - cur;
+      pp.pad = 0;
+      if (pp.active) cur = 1 - cur;
+      plan[p] = pp;
+    }
+    *d_sel = cur;
+  }
+}
+
+template <typename KeyT>
+struct PassSmem {
+  KeyT keys[kTile];
+  uint32_t vals[kTile];
+  uint32_t warp_hist[kSortWarps][kRadix];
+  uint32_t digit_start[kRadix];  // tile-local exclusive start of each digit
+  uint32_t global_start[kRadix];
+  uint32_t scan_tmp[kRadix];
+  int tile;
+};
+
+template <typename KeyT>
+__global__ void __launch_bounds__(kSortBlock) onesweep_pass(KeyT *keys0, uint32_t *vals0, KeyT *keys1,
+                                                           uint32_t *vals1, int64_t n, int shift,
+                                                           const PassPlan *__restrict__ plan,
+                                                           const uint32_t *__restrict__ goff,
+                                                           uint32_t *status, unsigned *tile_ticket,
+                                                           unsigned *err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PassSmem<KeyT> &S = *reinterpret_cast<PassSmem<KeyT> *>(smem_raw);
+  const PassPlan pp = *plan;
+  if (!pp.active) return;
+  const KeyT *src_k = pp.src ? keys1 : keys0;
+  const uint32_t *src_v = pp.src ? vals1 : vals0;
+  KeyT *dst_k = pp.dst ? keys1 : keys0;
+  uint32_t *dst_v = pp.dst ? vals1 : vals0;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) S.tile = (int)atomicAdd(tile_ticket, 1u);
+  for (int i = tid; i < kSortWarps * kRadix; i += kSortBlock) (&S.warp_hist[0][0])[i] = 0;
+  __syncthreads();
+  const int tile = S.tile;
+  const int64_t base = (int64_t)tile * kTile;
+  const int64_t wbase = base + (int64_t)warp * 32 * kItems;
+
+  KeyT k[kItems];
+  uint32_t v[kItems];
+  int dig[kItems];
+  uint32_t rank[kItems];
+#pragma unroll
+  for (int i = 0; i < kItems; i++) {
+    int64_t idx = wbase + i * 32 + lane;
+    if (idx < n) {
+      k[i] = src_k[idx];
+      v[i] = src_v[idx];
+      dig[i] = (int)((k[i] >> shift) & 0xFF);
+    } else {
+      k[i] = 0;
+      v[i] = 0;
+      dig[i] = kRadix + lane;  // unique: no peers, never counted
+    }
+  }
+  const uint32_t lt = lanemask_lt();
+  uint32_t *wh = S.warp_hist[warp];
+#pragma unroll
+  for (int i = 0; i < kItems; i++) {
+    uint32_t peers = __match_any_sync(0xffffffffu, dig[i]);
+    uint32_t cnt = dig[i] < kRadix ? wh[dig[i]] : 0u;
+    rank[i] = cnt + __popc(peers & lt);
+    __syncwarp();
+    if (dig[i] < kRadix && (peers & lt) == 0) wh[dig[i]] = cnt + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  // per digit: exclusive prefix over warps, tile total
+  const int d = tid;  // kSortBlock == kRadix
+  uint32_t total = 0;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; w++) {
+    uint32_t c = S.warp_hist[w][d];
+    S.warp_hist[w][d] = total;
+    total += c;
+  }
+  // tile-local exclusive scan over digits
+  S.scan_tmp[d] = total;
+  __syncthreads();
+  for (int o = 1; o < kRadix; o <<= 1) {
+    uint32_t t = d >= o ? S.scan_tmp[d - o] : 0u;
+    __syncthreads();
+    S.scan_tmp[d] += t;
+    __syncthreads();
+  }
+  S.digit_start[d] = S.scan_tmp[d] - total;
+
+  // decoupled look-back for digit d
+  uint32_t *st = status + (int64_t)tile * kRadix + d;
+  uint32_t excl;
+  if (tile == 0) {
+    excl = goff[d];
+    atomicExch(st, kFlagPrefix | ((excl + total) & kCountMask));
+  } else {
+    atomicExch(st, kFlagAgg | (total & kCountMask));
+    uint32_t acc = 0;
+    int t = tile - 1;
+    int spins = 0;
+    bool timed_out = false;
+    while (t >= 0) {
+      uint32_t s = *reinterpret_cast<volatile uint32_t *>(status + (int64_t)t * kRadix + d);
+      if ((s & ~kCountMask) == 0u) {
+        if (++spins > kSpinLimit) {
+          timed_out = true;
+          break;
+        }
+        continue;
+      }
+      acc += s & kCountMask;
+      if ((s & ~kCountMask) == kFlagPrefix) break;
+      t--;
+    }
+    if (t < 0) acc += goff[d];  // cannot happen: tile 0 always publishes a prefix
+    if (timed_out) atomicOr(err, kErrTimeout);
+    excl = acc;
+    atomicExch(st, kFlagPrefix | ((excl + total) & kCountMask));
+  }
+  S.global_start[d] = excl;
+  __syncthreads();
+
+  // stage in digit order
+#pragma unroll
+  for (int i = 0; i < kItems; i++) {
+    if (dig[i] < kRadix) {
+      uint32_t pos = S.digit_start[dig[i]] + S.warp_hist[warp][dig[i]] + rank[i];
+      S.keys[pos] = k[i];
+      S.vals[pos] = v[i];
+    }
+  }
+  __syncthreads();
+  int64_t valid = n - base;
+  if (valid > kTile) valid = kTile;
+  for (int i = tid; i < valid; i += kSortBlock) {
+    KeyT kk = S.keys[i];
+    int dd = (int)((kk >> shift) & 0xFF);
+    int64_t dst = (int64_t)S.global_start[dd] + (i - (int64_t)S.digit_start[dd]);
+    dst_k[dst] = kk;
+    dst_v[dst] = S.vals[i];
+  }
+}
+
+}  // namespace
+
+template <typename KeyT>
+int radix_sort_pairs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1, int64_t n, int key_bits,
+                     int *d_sel, unsigned *d_err, cudaStream_t s) {
+  PRT_CHECK(n >= 0 && n < (int64_t)kCountMask, PRT_ERR_INVALID, "radix sort: n=%lld out of range",
+            (long long)n);
+  int passes = (key_bits + 7) / 8;
+  if (passes < 1) passes = 1;
+  PRT_CHECK(passes <= (int)sizeof(KeyT), PRT_ERR_INVALID, "radix sort: %d key bits", key_bits);
+  if (n == 0) {
+    PRT_CUDA(cudaMemsetAsync(d_sel, 0, sizeof(int), s));
+    return PRT_OK;
+  }
+  const int64_t tiles = (n + kTile - 1) / kTile;
+  // scratch: hist, offsets, plan, tickets, status
+  size_t hist_b = sizeof(uint32_t) * passes * kRadix;
+  size_t plan_b = sizeof(PassPlan) * passes;
+  size_t tick_b = sizeof(unsigned) * passes;
+  size_t stat_b = sizeof(uint32_t) * (size_t)tiles * kRadix * passes;
+  unsigned char *scratch = nullptr;
+  size_t total = 2 * hist_b + plan_b + tick_b + stat_b + 256;
+  int rc = dmalloc(reinterpret_cast<void **>(&scratch), total, s);
+  if (rc) return rc;
+  uint32_t *ghist = reinterpret_cast<uint32_t *>(scratch);
+  uint32_t *goff = ghist + passes * kRadix;
+  PassPlan *plan = reinterpret_cast<PassPlan *>(goff + passes * kRadix);
+  unsigned *tick = reinterpret_cast<unsigned *>(plan + passes);
+  uint32_t *status = reinterpret_cast<uint32_t *>(tick + passes);
+  cudaError_t e = cudaMemsetAsync(scratch, 0, total, s);
+  if (e == cudaSuccess) {
+    int g = grid_for(n, 256, 4);
+    {
+      PRT_PROF("hist", s);
+      hist_kernel<KeyT><<<g, 256, sizeof(uint32_t) * passes * kRadix, s>>>(keys0, n, passes, ghist);
+    }
+    {
+      PRT_PROF("plan", s);
+      plan_kernel<<<1, kRadix, 0, s>>>(ghist, goff, passes, n, plan, d_sel);
+    }
+    size_t smem = sizeof(PassSmem<KeyT>);
+    e = cudaFuncSetAttribute(onesweep_pass<KeyT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    for (int p = 0; p < passes && e == cudaSuccess; p++) {
+      {
+        PRT_PROF("onesweep_pass", s);
+        onesweep_pass<KeyT><<<(unsigned)tiles, kSortBlock, smem, s>>>(
+          keys0, vals0, keys1, vals1, n, 8 * p, plan + p, goff + p * kRadix,
+          status + (size_t)p * tiles * kRadix, tick + p, d_err);
+      }
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+  }
+  dfree(scratch, s);
+  if (e != cudaSuccess) return cuda_status(e, "radix_sort_pairs");
+  return PRT_OK;
+}
+
+template int radix_sort_pairs<uint32_t>(uint32_t *, uint32_t *, uint32_t *, uint32_t *, int64_t, int, int *,
+                                        unsigned *, cudaStream_t);
+template int radix_sort_pairs<uint64_t>(uint64_t *, uint32_t *, uint64_t *, uint32_t *, int64_t, int, int *,
+                                        unsigned *, cudaStream_t);
+
+}  // namespace prt
