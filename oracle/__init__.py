@@ -254,12 +254,14 @@ def ref_gpc_clip(subj, clip, op: int = 1):
 
 
 def result_area(contours) -> float:
-    total = 0.0
-    for hole, v in contours:
-        x, y = v[:, 0], v[:, 1]
-        a = 0.5 * abs(float(np.dot(x, np.roll(y, -1)) - np.dot(np.roll(x, -1), y)))
-        total += -a if hole else a
-    return total
+    """Sum of |shoelace| over contours (holes negative), by the C oracle
+    (coordinates relative to each contour's first vertex)."""
+    if not contours:
+        return 0.0
+    nv = np.array([len(v) for _, v in contours], dtype=np.int32)
+    hole = np.array([h for h, _ in contours], dtype=np.int32)
+    xy = np.ascontiguousarray(np.concatenate([v for _, v in contours]), dtype=np.float64)
+    return float(lib().orc_result_area(C.c_int(len(contours)), _p(nv), _p(hole), _p(xy)))
 
 
 def area_grad(subj, clip, subj_hole=None, clip_hole=None):

@@ -837,16 +837,21 @@ int orc_gpc_clip(int op, int s_ncont, const int *s_nverts, const double *s_xy,
 
 /* ---- area of a result ------------------------------------------------------ */
 
-/* Sum over contours of |shoelace area|, negated for hole contours. */
+/* Sum over contours of |shoelace area|, negated for hole contours.  The
+ * shoelace runs on coordinates relative to the contour's first vertex: for
+ * small contours far from the origin the plain form cancels terms of size
+ * |x||y| down to an area of size r^2 and loses ~|x||y|/r^2 ulps. */
 double orc_result_area(int ncont, const int *nverts, const int *hole, const double *xy) {
   double total = 0.0;
   int64_t off = 0;
   for (int c = 0; c < ncont; c++) {
     int n = nverts[c];
     double a = 0.0;
+    const double x0 = xy[2 * off], y0 = xy[2 * off + 1];
     for (int i = 0; i < n; i++) {
       int j = (i + 1) % n;
-      a += xy[2 * (off + i)] * xy[2 * (off + j) + 1] - xy[2 * (off + j)] * xy[2 * (off + i) + 1];
+      a += (xy[2 * (off + i)] - x0) * (xy[2 * (off + j) + 1] - y0) -
+           (xy[2 * (off + j)] - x0) * (xy[2 * (off + i) + 1] - y0);
     }
     a = 0.5 * fabs(a);
     total += hole[c] ? -a : a;

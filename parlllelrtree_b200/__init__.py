@@ -316,7 +316,7 @@ def clip_pair(subj, clip, op: str = "int"):
         oxy = np.zeros((cap_v, 2), np.float64)
         rc = lib().prt_clip_pair_host(OP[op], sn, p(snv), p(sxy), cn, p(cnv), p(cxy), C.byref(oc), cap_c, p(onv),
                                       p(oh), C.byref(ov), cap_v, p(oxy))
-        if rc == _lib.PRT_ERR_CAPACITY:
+        if rc == _lib.PRT_ERR_CAPACITY and (oc.value > cap_c or ov.value > cap_v):
             cap_c, cap_v = max(cap_c, oc.value), max(cap_v, ov.value)
             continue
         check(rc)

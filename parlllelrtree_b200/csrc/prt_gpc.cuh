@@ -968,21 +968,31 @@ __device__ inline void write_result(const Arena &A, int out_poly, int32_t *cont_
   }
 }
 
-// Sum over result contours of |shoelace area|, hole contours negative.
+// Sum over result contours of |shoelace area|, hole contours negative.  The
+// shoelace runs on coordinates relative to the contour's first output vertex
+// (the last node of its left-to-right list): the plain form cancels terms of
+// size |x||y| down to an area of size r^2 and loses ~|x||y|/r^2 ulps on small
+// contours far from the origin.  Terms are summed in list order (the reverse
+// of output order), so the value agrees with a sum over the written-out
+// contour to rounding (~1e-15 relative), not bit for bit.
 __device__ inline double result_area(const Arena &A, int out_poly) {
   double total = 0.0;
   for (int p = out_poly; p >= 0; p = A.P[p].next) {
     if (!A.P[p].active) continue;
     const int px2 = A.P[p].proxy;
-    int v = A.P[px2].vl;
-    const double x0 = A.V[v].x, y0 = A.V[v].y;
-    double a = 0.0, xp = x0, yp = y0;
-    for (v = A.V[v].next; v >= 0; v = A.V[v].next) {
-      a += xp * A.V[v].y - A.V[v].x * yp;
-      xp = A.V[v].x;
-      yp = A.V[v].y;
+    int last = A.P[px2].vl;
+    while (A.V[last].next >= 0) last = A.V[last].next;
+    const double x0 = A.V[last].x, y0 = A.V[last].y;
+    // the walk visits output vertices n-1, n-2, ..., 0; the term of output
+    // edge (i, i+1) pairs the visited vertex i with the one visited before it
+    double xn = 0.0, yn = 0.0;  // output vertex 0, relative to itself
+    double a = 0.0;
+    for (int u = A.P[px2].vl; u >= 0; u = A.V[u].next) {
+      const double xi = A.V[u].x - x0, yi = A.V[u].y - y0;
+      a += xi * yn - xn * yi;
+      xn = xi;
+      yn = yi;
     }
-    a += xp * y0 - x0 * yp;
     a = 0.5 * fabs(a);
     total += A.P[px2].hole ? -a : a;
   }

@@ -95,6 +95,9 @@ __device__ void process_pair(const PairSrc &S, const ClipOut &O, int64_t i, unsi
     cbase = (int64_t)atomicAdd(&O.pool[0], (unsigned long long)nc);
     vbase = (int64_t)atomicAdd(&O.pool[1], (unsigned long long)nvt);
     if (cbase + nc > O.cap_c || vbase + nvt > O.cap_v) {
+      // record what the pair needs so the host grows the pools enough
+      O.pair_ncont[i] = nc;
+      O.pair_cstart[i] = nvt;
       O.status[i] = kPairPool;
       return;
     }
@@ -194,14 +197,39 @@ __global__ void area_from_results_kernel(const int64_t *__restrict__ pair_cstart
       const double *v = xy + 2 * cont_vstart[cc];
       int m = cont_nverts[cc];
       double a = 0.0;
+      // relative to the first vertex, in output order (as the oracle sums)
+      const double x0 = v[0], y0 = v[1];
       for (int j = 0; j < m; j++) {
         int k = (j + 1) % m;
-        a += v[2 * j] * v[2 * k + 1] - v[2 * k] * v[2 * j + 1];
+        a += (v[2 * j] - x0) * (v[2 * k + 1] - y0) - (v[2 * k] - x0) * (v[2 * j + 1] - y0);
       }
       a = 0.5 * fabs(a);
       total += cont_hole[cc] ? -a : a;
     }
     area[i] = total;
+  }
+}
+
+// contours, vertices and non-empty pairs over the live results
+__global__ void result_totals_kernel(const int64_t *__restrict__ pair_cstart, const int32_t *__restrict__ pair_ncont,
+                                     const int32_t *__restrict__ cont_nverts, int64_t n,
+                                     unsigned long long *__restrict__ tot) {
+  unsigned long long c = 0, v = 0, ne = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int k = pair_ncont[i];
+    c += k;
+    ne += k > 0;
+    for (int j = 0; j < k; j++) v += cont_nverts[pair_cstart[i] + j];
+  }
+  for (int o = 16; o; o >>= 1) {
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+    ne += __shfl_xor_sync(0xffffffffu, ne, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&tot[0], c);
+    atomicAdd(&tot[1], v);
+    atomicAdd(&tot[2], ne);
   }
 }
 
@@ -418,15 +446,23 @@ static int run_batched(OverlayState &st, cudaStream_t s) {
 static int retry_failed(OverlayState &st, cudaStream_t s) {
   const int64_t n = st.n;
   std::vector<int32_t> hs(n);
-  for (int round = 0; round < 6; round++) {
+  std::vector<int32_t> scale(n, 1);  // arena scale per pair: x4 after each arena overflow
+  for (int round = 0; round < 8; round++) {
     PRT_CUDA(cudaMemcpyAsync(hs.data(), st.O.status, 4 * n, cudaMemcpyDeviceToHost, s));
     PRT_CUDA(cudaStreamSynchronize(s));
-    std::vector<int64_t> fail;
-    bool pool = false;
+    std::vector<int64_t> pool_fail;
+    bool any = false;
     for (int64_t i = 0; i < n; i++) {
-      if (hs[i] == kPairArena || hs[i] == kPairPool) {
-        fail.push_back(i);
-        pool |= hs[i] == kPairPool;
+      if (hs[i] == kPairArena) {
+        if (scale[i] >= (1 << 12)) {
+          set_error("overlay: pair %lld exceeds the largest arena slice", (long long)i);
+          return PRT_ERR_CAPACITY;
+        }
+        scale[i] *= 4;
+        any = true;
+      } else if (hs[i] == kPairPool) {
+        pool_fail.push_back(i);
+        any = true;
       } else if (hs[i] == kPairInvalid) {
         set_error("overlay: pair %lld names a polygon outside its layer", (long long)i);
         return PRT_ERR_INVALID;
@@ -435,21 +471,43 @@ static int retry_failed(OverlayState &st, cudaStream_t s) {
         return PRT_ERR_INVALID;
       }
     }
-    if (fail.empty()) return PRT_OK;
-    st.retried += (int64_t)fail.size();
-    if (pool) {
-      int rc = grow_pools(st, s, 0, 0);
+    if (!any) return PRT_OK;
+    if (!pool_fail.empty()) {
+      // the failing pairs recorded their needs in pair_ncont / pair_cstart
+      std::vector<int32_t> nc(n);
+      std::vector<int64_t> nvt(n);
+      PRT_CUDA(cudaMemcpyAsync(nc.data(), st.O.pair_ncont, 4 * n, cudaMemcpyDeviceToHost, s));
+      PRT_CUDA(cudaMemcpyAsync(nvt.data(), st.O.pair_cstart, 8 * n, cudaMemcpyDeviceToHost, s));
+      PRT_CUDA(cudaStreamSynchronize(s));
+      int64_t need_c = 0, need_v = 0;
+      for (int64_t i : pool_fail) {
+        need_c += nc[i];
+        need_v += nvt[i];
+      }
+      int rc = grow_pools(st, s, need_c, need_v);
       if (rc) return rc;
     }
-    int64_t *d_idx = nullptr;
-    int rc = dalloc(&d_idx, fail.size(), s);
-    if (rc) return rc;
-    cudaMemcpyAsync(d_idx, fail.data(), 8 * fail.size(), cudaMemcpyHostToDevice, s);
-    rc = run_plain(st, d_idx, (int64_t)fail.size(), 1 << (2 * (round + 1)), s);
-    dfree(d_idx, s);
-    if (rc) return rc;
+    // rerun every failed pair, grouped by arena scale
+    std::vector<int32_t> scales;
+    for (int64_t i = 0; i < n; i++)
+      if (hs[i] == kPairArena || hs[i] == kPairPool) scales.push_back(scale[i]);
+    std::sort(scales.begin(), scales.end());
+    scales.erase(std::unique(scales.begin(), scales.end()), scales.end());
+    for (int32_t sc : scales) {
+      std::vector<int64_t> idx;
+      for (int64_t i = 0; i < n; i++)
+        if ((hs[i] == kPairArena || hs[i] == kPairPool) && scale[i] == sc) idx.push_back(i);
+      st.retried += (int64_t)idx.size();
+      int64_t *d_idx = nullptr;
+      int rc = dalloc(&d_idx, idx.size(), s);
+      if (rc) return rc;
+      cudaMemcpyAsync(d_idx, idx.data(), 8 * idx.size(), cudaMemcpyHostToDevice, s);
+      rc = run_plain(st, d_idx, (int64_t)idx.size(), sc, s);
+      dfree(d_idx, s);
+      if (rc) return rc;
+    }
   }
-  set_error("overlay: pairs still exceed the largest arena after retries");
+  set_error("overlay: pairs still failing after retries");
   return PRT_ERR_CAPACITY;
 }
 
@@ -548,25 +606,27 @@ int overlay_impl(const PairSrc &S, int64_t n, int sched, double *d_area, cudaStr
   r->cont_hole = st.O.cont_hole;
   r->xy = st.O.xy;
   r->pool = st.O.pool;
-  // exact totals from the per-pair counts
+  // exact totals of the live results (pools may hold abandoned reservations)
   {
-    std::vector<int32_t> nc(n);
-    cudaError_t e = cudaMemcpyAsync(nc.data(), r->pair_ncont, 4 * n, cudaMemcpyDeviceToHost, s);
+    unsigned long long *tot = nullptr;
+    int rc2 = dalloc(&tot, 3, s);
+    unsigned long long h[3] = {0, 0, 0};
+    cudaError_t e = rc2 ? cudaErrorMemoryAllocation : cudaMemsetAsync(tot, 0, 24, s);
+    if (e == cudaSuccess && n > 0) {
+      PRT_PROF("result_totals", s);
+      result_totals_kernel<<<grid_for(n, 256, 8), 256, 0, s>>>(r->pair_cstart, r->pair_ncont, r->cont_nverts, n, tot);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, tot, sizeof h, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    dfree(tot, s);
     if (e != cudaSuccess) {
       prt_results_free(r);
       return cuda_status(e, "overlay results");
     }
-    int64_t c = 0, ne = 0;
-    for (int64_t i = 0; i < n; i++) {
-      c += nc[i];
-      ne += nc[i] > 0;
-    }
-    r->n_cont = c;
-    r->nonempty = ne;
-    unsigned long long used[2];
-    cudaMemcpy(used, r->pool, sizeof used, cudaMemcpyDeviceToHost);
-    r->n_vert = (int64_t)used[1];
+    r->n_cont = (int64_t)h[0];
+    r->n_vert = (int64_t)h[1];
+    r->nonempty = (int64_t)h[2];
   }
   *out = r;
   return PRT_OK;

@@ -38,3 +38,30 @@ def test_no_device_is_reported_not_faked():
     n = L.prt_device_count()
     assert n >= 0
     assert L.prt_version() == 1
+
+
+def test_bad_arguments_are_rejected_before_any_device_work():
+    from parlllelrtree_b200 import _lib
+
+    L = _lib.lib()
+    tree = ctypes.c_void_p()
+    # fanout out of range, null boxes, unknown key mode, REF64 on float boxes
+    assert L.prt_build_bottomup(ctypes.c_void_p(16), 1, None, 100, 1, 1, None, ctypes.byref(tree)) == _lib.PRT_ERR_INVALID
+    assert L.prt_build_bottomup(None, 1, None, 100, 16, 1, None, ctypes.byref(tree)) == _lib.PRT_ERR_INVALID
+    assert L.prt_build_bottomup(ctypes.c_void_p(16), 1, None, 100, 16, 7, None, ctypes.byref(tree)) == _lib.PRT_ERR_INVALID
+    assert L.prt_build_bottomup(ctypes.c_void_p(16), 1, None, 100, 16, 0, None, ctypes.byref(tree)) == _lib.PRT_ERR_INVALID
+    assert b"REF64" in L.prt_last_error()
+    assert L.prt_tree_info(None, None) == _lib.PRT_ERR_INVALID
+
+
+def test_without_a_device_compute_fails_loudly():
+    """No CPU fallback: with no CUDA device a build returns PRT_ERR_CUDA/NOMEM."""
+    from parlllelrtree_b200 import _lib
+
+    L = _lib.lib()
+    if L.prt_device_count() > 0:
+        return  # on a GPU box this case cannot be produced
+    tree = ctypes.c_void_p()
+    rc = L.prt_build_bottomup(ctypes.c_void_p(256), 1, None, 100, 16, 1, None, ctypes.byref(tree))
+    assert rc in (_lib.PRT_ERR_CUDA, _lib.PRT_ERR_NOMEM)
+    assert L.prt_last_error()

@@ -57,30 +57,65 @@ def test_forward_and_adjoint_match_oracle(cuda, hole_frac):
         assert np.abs(gb[vb] - wn[i] * rc).max() <= 1e-9 * wn[i] * scale, i
 
 
-def test_adjoint_matches_finite_differences(cuda):
-    import parlllelrtree_b200 as prt
-
-    n = 6
-    A, B = overlapping_pairs(n, seed=17)
+def _fd_check(prt, A, B, n, h=1e-6):
+    """Central differences (h = 1e-6) of the device forward area against the
+    adjoint, coordinate by coordinate.  The area is piecewise smooth: it has
+    a kink wherever a vertex crosses the other polygon's boundary, and on
+    polygons of radius ~1e-3 a stencil of +-1e-6 straddles one for a few
+    percent of the vertices.  A coordinate whose one-sided slopes disagree by
+    more than 1e-3 of the gradient scale is such a case: there the adjoint
+    must lie between the two one-sided slopes.  Everywhere else the central
+    difference must match it to 1e-5 of the gradient scale (truncation
+    h^2 f'''/6 ~ 1e-12 / r reaches ~1e-6 relative at r = 1e-3) plus half the
+    one-sided disagreement (a milder kink inside the stencil)."""
     LA, LB = prt.Layer.from_dict(A), prt.Layer.from_dict(B)
     idx = torch.arange(n, dtype=torch.int32, device="cuda")
     xa = LA.xy.clone().requires_grad_(True)
     prt.intersection_area(LA, LB, idx, idx, xa, LB.xy).sum().backward()
     g = xa.grad.cpu().numpy()
-    h = 1e-6
+    scale = np.abs(g).max()
     x0 = LA.xy.clone()
-    fd = np.zeros_like(g)
+    f0 = prt.intersection_area(LA, LB, idx, idx, x0, LB.xy).sum().item()
+    smooth = kinked = 0
     for v in range(len(g)):
         for d in range(2):
             xp = x0.clone()
             xp[v, d] += h
             xm = x0.clone()
             xm[v, d] -= h
-            ap = prt.intersection_area(LA, LB, idx, idx, xp, LB.xy).sum().item()
-            am = prt.intersection_area(LA, LB, idx, idx, xm, LB.xy).sum().item()
-            fd[v, d] = (ap - am) / (2 * h)
-    # central differences, h = 1e-6: error ~ h^2 |f'''| + eps |area| / h
-    assert np.abs(fd - g).max() <= 1e-6 * np.abs(g).max() + 1e-9
+            fp = prt.intersection_area(LA, LB, idx, idx, xp, LB.xy).sum().item()
+            fm = prt.intersection_area(LA, LB, idx, idx, xm, LB.xy).sum().item()
+            dp, dm = (fp - f0) / h, (f0 - fm) / h
+            if abs(dp - dm) <= 1e-3 * scale:
+                smooth += 1
+                assert abs((fp - fm) / (2 * h) - g[v, d]) <= 1e-5 * scale + 0.5 * abs(dp - dm), (v, d)
+            else:
+                kinked += 1
+                lo, hi = min(dp, dm), max(dp, dm)
+                assert lo - 1e-6 * scale <= g[v, d] <= hi + 1e-6 * scale, (v, d)
+    return smooth, kinked
+
+
+def test_adjoint_matches_finite_differences(cuda):
+    import parlllelrtree_b200 as prt
+
+    A, B = overlapping_pairs(6, seed=17)  # radius log-uniform 1e-3..1e-2
+    smooth, kinked = _fd_check(prt, A, B, 6)
+    assert smooth >= 0.9 * (smooth + kinked)
+
+
+def test_adjoint_matches_finite_differences_large(cuda):
+    """Radius 0.05: kinks inside a 1e-6 stencil become rare."""
+    import parlllelrtree_b200 as prt
+
+    n = 4
+    rng = np.random.default_rng(29)
+    c = rng.random((n, 2)) * 0.5 + 0.25
+    r = np.full(n, 0.05)
+    A = dg.star_layer(n, seed=30, nv_lo=16, nv_hi=40, centre_xy=c, radii=r)
+    B = dg.star_layer(n, seed=31, nv_lo=16, nv_hi=40, centre_xy=c + 0.02, radii=r)
+    smooth, kinked = _fd_check(prt, A, B, n)
+    assert smooth >= 0.98 * (smooth + kinked)
 
 
 def test_shared_polygons_accumulate(cuda):

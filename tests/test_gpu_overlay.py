@@ -164,5 +164,6 @@ def test_results_area_matches_oracle(cuda):
     res = prt.overlay(torch.from_numpy(pairs).cuda(), prt.Layer.from_dict(A), prt.Layer.from_dict(B))
     area = res.area().cpu().numpy()
     for k, (i, j) in enumerate(pairs):
+        # same contours, same centred shoelace in the same order as the oracle
         ref = oracle.result_area(oracle.gpc_clip(rings_of(A, i), rings_of(B, j), 1))
-        assert abs(area[k] - ref) <= 1e-12 * abs(ref) + 1e-20
+        assert abs(area[k] - ref) <= 1e-12 * abs(ref) + 1e-24
