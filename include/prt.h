@@ -148,7 +148,21 @@ int prt_tree_export_td(const prt_tree *t, int32_t *h_nodes_index, double *h_node
 int prt_join(const prt_tree *t, const void *d_queries, int coord_type, int64_t nq,
              prt_pair *d_pairs, int64_t cap, int64_t *h_count, void *stream);
 
-/* Same, with the pairs sorted by (queryid, nodeid). */
+/* prt_join without any device allocation (no counterpart in the reference).
+ * For callers that cannot allocate device memory when they join: inside a
+ * CUDA stream capture, under a host process that owns the whole device memory
+ * budget through its own pool, or in a loop that cannot afford the device
+ * synchronisation an allocation may cause.  The frontier scratch lives in a
+ * fixed array of the library (64 MiB + 512 B, reserved on every GPU that loads
+ * the library): a level frontier above 4,194,304 (query, node) items returns
+ * PRT_ERR_CAPACITY with a message, as does a pair count above `cap` (the count
+ * is still reported).  The first call on a device looks the array up, so make
+ * it before any stream capture.  Calls share the array: calls that can overlap
+ * on the GPU race and must be serialised by the caller. */
+int prt_join_noalloc(const prt_tree *t, const void *d_queries, int coord_type, int64_t nq,
+                     prt_pair *d_pairs, int64_t cap, int64_t *h_count, void *stream);
+
+/* Same as prt_join, with the pairs sorted by (queryid, nodeid). */
 int prt_join_sorted(const prt_tree *t, const void *d_queries, int coord_type, int64_t nq,
                     prt_pair *d_pairs, int64_t cap, int64_t *h_count, void *stream);
 

@@ -42,6 +42,7 @@ _SIGS = {
     "prt_tree_export_td": (_I, [_P, _P, _P, _P]),
     "prt_join": (_I, [_P, _P, _I, _I64, _P, _I64, _P, _P]),
     "prt_join_sorted": (_I, [_P, _P, _I, _I64, _P, _I64, _P, _P]),
+    "prt_join_noalloc": (_I, [_P, _P, _I, _I64, _P, _I64, _P, _P]),
     "prt_query_counts": (_I, [_P, _P, _I, _I64, _I, _P, _P]),
     "prt_overlay_run": (_I, [_P, _I64, C.c_int32, _P, _P, _P, _I, _I, _P, _P]),
     "prt_overlay_run_ref": (_I, [_P, _I64, C.c_int32, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _P, _I64, _I, _I,

@@ -289,3 +289,128 @@ int prt_query_counts(const prt_tree *t, const void *d_queries, int coord_type, i
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free join.
+//
+// prt_join takes its frontier buffers and level counters from the
+// stream-ordered allocator.  Some callers cannot allocate device memory at
+// the moment they join: a caller in the middle of a CUDA stream capture (the
+// graph would record the allocation, or the capture mode forbids it), a host
+// process that hands the whole device budget to its own pool and treats any
+// other allocation as a failure, or a latency-critical loop that cannot take
+// the device synchronisation cudaMalloc/cudaFree may imply.  prt_join_noalloc
+// runs the same breadth-first traversal with its scratch in the file-scope
+// array below instead: the caller passes the queries and the pair buffer,
+// and the library allocates nothing.
+//
+// The array is reserved on every GPU that loads the library, for the life of
+// the process.  Its device address is looked up once per device
+// (cudaGetSymbolAddress, with that device current) on the first call made
+// there, so make that first call before any stream capture.  All calls on a
+// device share the one array: calls that can overlap on the GPU (different
+// streams, or host threads) race on it and must be serialised by the caller.
+#include <mutex>
+
+namespace prt {
+namespace {
+
+// Frontier items per buffer: two (query, node) buffers of 4 Mi items each
+// (64 MiB) plus the level counters.
+constexpr int64_t kNoAllocFrontier = 1ll << 22;
+constexpr size_t kNoAllocCounterBytes = 512;  // 64 x uint64, room for PRT_MAX_LEVELS + 2
+constexpr size_t kNoAllocBytes = kNoAllocCounterBytes + 2 * sizeof(uint2) * (size_t)kNoAllocFrontier;
+
+static __device__ __align__(256) unsigned char g_join_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_addr[256] = {nullptr};  // per device, set on first use
+
+int noalloc_scratch(unsigned char **out) {
+  int dev = 0;
+  PRT_CUDA(cudaGetDevice(&dev));
+  PRT_CHECK(dev >= 0 && dev < 256, PRT_ERR_INVALID, "device %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_join_scratch);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(join scratch)");
+    g_noalloc_addr[dev] = reinterpret_cast<unsigned char *>(p);
+  }
+  *out = g_noalloc_addr[dev];
+  return PRT_OK;
+}
+
+}  // namespace
+}  // namespace prt
+
+extern "C" {
+
+int prt_join_noalloc(const prt_tree *t, const void *d_queries, int coord_type, int64_t nq, prt_pair *d_pairs,
+                     int64_t cap, int64_t *h_count, void *stream) {
+  using namespace prt;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  PRT_CHECK(t != nullptr, PRT_ERR_INVALID, "tree is NULL");
+  PRT_CHECK(coord_type == t->coord, PRT_ERR_INVALID, "query coordinate type %d differs from the tree's %d",
+            coord_type, t->coord);
+  PRT_CHECK(nq >= 0 && nq < (1ll << 31), PRT_ERR_INVALID, "nq=%lld", (long long)nq);
+  PRT_CHECK(cap >= 0 && (cap == 0 || d_pairs != nullptr), PRT_ERR_INVALID, "pair buffer");
+  PRT_CHECK(t->lv.levels + 2 <= (int)(kNoAllocCounterBytes / 8), PRT_ERR_INVALID, "tree too deep");
+  if (h_count) *h_count = 0;
+  if (nq == 0) return PRT_OK;
+  unsigned char *scr = nullptr;
+  int rc = noalloc_scratch(&scr);
+  if (rc) return rc;
+  unsigned long long *cnt = reinterpret_cast<unsigned long long *>(scr);
+  uint2 *fr[2] = {reinterpret_cast<uint2 *>(scr + kNoAllocCounterBytes),
+                  reinterpret_cast<uint2 *>(scr + kNoAllocCounterBytes) + kNoAllocFrontier};
+  // the counters must start at zero; the frontier buffers are written before read
+  PRT_CUDA(cudaMemsetAsync(cnt, 0, kNoAllocCounterBytes, s));
+  const TreeLevels &L = t->lv;
+  const size_t bs = 4 * coord_size(t->coord);
+  const int leaf_slot = PRT_MAX_LEVELS;  // counter of emitted pairs
+  int cur = -1;
+  for (int l = L.levels - 1; l >= 0 && !rc; l--) {
+    JoinLevel J;
+    J.mbr = reinterpret_cast<const char *>(t->d_mbr) + L.offset[l] * bs;
+    J.n_entries = L.count[l];
+    J.in = cur < 0 ? nullptr : fr[cur];
+    J.in_count = cur < 0 ? nullptr : &cnt[l + 1];
+    J.in_cap = kNoAllocFrontier;
+    J.leaf = l == 0;
+    int nxt = cur < 0 ? 0 : 1 - cur;
+    J.out = J.leaf ? reinterpret_cast<uint2 *>(d_pairs) : fr[nxt];
+    J.out_count = J.leaf ? &cnt[leaf_slot] : &cnt[l];
+    J.out_cap = J.leaf ? cap : kNoAllocFrontier;
+    J.nq = nq;
+    J.counts = nullptr;
+    J.td_slots = 0;
+    rc = dispatch_coord(t->coord, [&](auto tag) {
+      using T = decltype(tag);
+      return launch_expand<T>(J, d_queries, t->fanout, s);
+    });
+    cur = nxt;
+  }
+  if (rc) return rc;
+  PRT_CUDA(cudaGetLastError());
+  unsigned long long h[PRT_MAX_LEVELS + 2];
+  PRT_CUDA(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, s));
+  PRT_CUDA(cudaStreamSynchronize(s));
+  for (int l = 1; l < L.levels; l++) {
+    if ((int64_t)h[l] > kNoAllocFrontier) {
+      set_error("prt_join_noalloc: a frontier of %llu (query, node) items exceeds the fixed scratch of %lld items; "
+                "use prt_join or fewer queries per call",
+                h[l], (long long)kNoAllocFrontier);
+      return PRT_ERR_CAPACITY;
+    }
+  }
+  const int64_t np = (int64_t)h[leaf_slot];
+  if (h_count) *h_count = np;
+  if (np > cap) {
+    set_error("prt_join_noalloc: %lld pairs exceed capacity %lld", (long long)np, (long long)cap);
+    return PRT_ERR_CAPACITY;
+  }
+  return PRT_OK;
+}
+
+}  // extern "C"
