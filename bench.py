@@ -46,7 +46,7 @@ WORKLOAD = "rtree_build_10M_f32_mixture64_bottomup_f16_morton32"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements")
@@ -85,19 +85,25 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t_end = time.perf_counter() + 5.0
+            while not self.lines and time.perf_counter() < t_end:  # sampler running before timing starts
+                time.sleep(0.01)
         except Exception:
             self.proc = None
+        self.t0 = time.perf_counter()
         return self
 
     def _read(self):
         for ln in self.proc.stdout:
-            self.lines.append(ln.strip())
+            self.lines.append((time.perf_counter(), ln.strip()))
 
     def __exit__(self, *a):
+        self.t1 = time.perf_counter()
         if self.proc:
+            time.sleep(0.06)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -107,7 +113,10 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        # samples taken while the timed steps ran (plus one sampling period)
+        for ts, ln in self.lines:
+            if not (self.t0 <= ts <= self.t1 + 0.06):
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 7:
                 continue
@@ -168,6 +177,7 @@ def time_steps(fn, steps, warmup, flush, world, before=None, after=None):
         ms.append(a.elapsed_time(b))
         if after:
             after(r)
+        del r  # the step's outputs are released outside the timed window
     barrier(world)
     torch.cuda.synchronize()
     return ms, time.perf_counter() - t0
@@ -191,7 +201,7 @@ def run_reference(args):
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's CPU code) is not built"}))
         return
-    sample = 2_000_000
+    sample = 1_000_000
     rects = dg.quantise(dg.mixture_boxes(N_BOXES, seed=0))
     for _ in range(args.warmup):
         reference_cpu_build(rects[:sample])
@@ -240,16 +250,27 @@ def run_ours(args):
     def drop(t):
         del t
 
-    # main timed region: profiled launches, clocks sampled
-    _lib.profile_enable(False)
+    # warm-up, then one untimed step with every launch timed (kernel shares
+    # and the dominant kernel), then the timed steps with launches counted and
+    # only the dominant kernel bracketed by events (on its launching stream)
+    _lib.profile_enable(0)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     _lib.profile_reset()
-    _lib.profile_enable(True)
+    _lib.profile_enable(1)
+    flush()
+    step()
+    torch.cuda.synchronize()
+    _lib.profile_enable(0)
+    shares = _lib.profile_read()
+    _lib.profile_reset()
+    dom_name = max(shares.items(), key=lambda kv: kv[1][0])[0]
+    _lib.profile_focus(dom_name)
+    _lib.profile_enable(2)
     with ClockSampler(local) as clk:
         ms, wall = time_steps(step, args.steps, 0, flush, world)
-    _lib.profile_enable(False)
+    _lib.profile_enable(0)
     prof = _lib.profile_read()
     _lib.profile_reset()
     mean_ms = float(np.mean(ms))
@@ -269,11 +290,10 @@ def run_ours(args):
     e2e = N_BOXES * world / (t_e2e * 1e-3) / 1e6
     top_levels = prt.build_bottomup(boxes, fanout=FANOUT).level_counts[-1]
 
-    # roofline of the dominant kernel
-    total = sum(v[0] for v in prof.values()) or 1.0
-    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    # roofline of the dominant kernel, timed live in the timed steps
+    total = sum(v[0] for v in shares.values()) or 1.0
     peak, peak_kind = hbm_peak()
-    dom_name, (dom_ms, dom_n) = dom
+    dom_ms, dom_n = prof.get(dom_name, (0.0, 0))
     per_launch_ms = dom_ms / max(dom_n, 1)
     algo_bytes = {
         # one radix pass moves every (key, value): read 4 + 4 B, write 4 + 4 B
@@ -309,7 +329,7 @@ def run_ours(args):
         "e2e": {"value": e2e, "unit": "Mboxes/s", "h2d_bytes_per_step": int(boxes_h.nbytes),
                 "d2h_bytes_per_step": int(top_levels * 32)},
         "gpu_launches": int(sum(v[1] for v in prof.values())),
-        "kernel_share": {k: round(v[0] / total, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+        "kernel_share": {k: round(v[0] / total, 4) for k, v in sorted(shares.items(), key=lambda kv: -kv[1][0])},
         "roofline": roofline,
         "clocks": clk.summary(),
         "wall_s_timed": wall,
@@ -405,6 +425,44 @@ def secondary(prt, boxes, flush, world):
                                              torch.arange(10000, device="cuda")))
     res["area_fwd_10k_pairs_s"] = 10000 / (ms * 1e-3)
     return res
+
+
+def batched_overlay(prt, scale: float = 1.0):
+    """The batched uneven overlay configuration: two layers of `scale` x 1M
+    star polygons (vertex count clip(Zipf(1.2), 4, 4096), 5% with 1-3 clockwise
+    holes, centres from the 64-Gaussian mixture, radius log-uniform
+    6.5e-5..6.5e-4, calibrated for ~4M candidate pairs at 1M x 1M), generated
+    on the device; tree over layer A's MBRs (fanout 16), join layer B, clip
+    every candidate pair once with the plain and once with the batched
+    schedule (CUDA events)."""
+    import torch
+    from parlllelrtree_b200 import datagen as dg
+
+    n = int(1_000_000 * scale)
+    A = dg.star_layer_device(n, seed=101, r_lo=6.5e-5, r_hi=6.5e-4)
+    B = dg.star_layer_device(n, seed=102, r_lo=6.5e-5, r_hi=6.5e-4)
+    LA, LB = prt.Layer.from_dict(A), prt.Layer.from_dict(B)
+    t = prt.build_bottomup(LA.mbr(), fanout=16)
+    pairs = t.join(LB.mbr())
+    l2p = t.leaf_order()
+    out = {"polygons_per_layer": n, "vertices_per_layer": [int(len(A["xy"])), int(len(B["xy"]))],
+           "pairs": int(len(pairs))}
+    for sched in ("batched", "plain"):
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        r = prt.overlay(pairs, LA, LB, leaf_to_poly=l2p, sched=sched)
+        b.record()
+        b.synchronize()
+        ms = a.elapsed_time(b)
+        out[f"{sched}_ms"] = ms
+        out[f"{sched}_pairs_s"] = len(pairs) / (ms * 1e-3)
+        out[f"{sched}_nonempty"] = r.nonempty
+        out[f"{sched}_retried"] = r.retried
+        del r
+    out["batched_over_plain"] = out["batched_pairs_s"] / out["plain_pairs_s"]
+    return out
 
 
 def main():

@@ -249,11 +249,14 @@ int prt_area_bwd(const int32_t *d_pair_a, const int32_t *d_pair_b, int64_t n_pai
 
 /* ---------------------------------------------------------------- profiling */
 
-/* Kernel launch profiler (no reference counterpart): when enabled, every
- * library kernel launch is bracketed by CUDA events on its stream.
- * prt_profile_read returns the number of kernel names (up to cap) and writes
- * newline-separated names, summed device milliseconds and launch counts. */
-int prt_profile_enable(int on);
+/* Kernel launch profiler (no reference counterpart).  Mode 1: every library
+ * kernel launch is bracketed by CUDA events on its stream; mode 2: launches
+ * are only counted, except those of the kernel named by prt_profile_focus,
+ * which are timed; 0: off.  prt_profile_read returns the number of kernel
+ * names (up to cap) and writes newline-separated names, summed device
+ * milliseconds (0 for counted-only kernels) and launch counts. */
+int prt_profile_enable(int mode);
+int prt_profile_focus(const char *kernel_name);
 int prt_profile_reset(void);
 int prt_profile_read(char *names, int names_cap, double *ms_total, int64_t *launches, int cap);
 

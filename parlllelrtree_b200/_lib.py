@@ -56,13 +56,20 @@ _SIGS = {
     "prt_area_fwd": (_I, [_P, _P, _I64, _P, _P, _P, _P]),
     "prt_area_bwd": (_I, [_P, _P, _I64, _P, _P, _P, _P, _P, _P]),
     "prt_profile_enable": (_I, [_I]),
+    "prt_profile_focus": (_I, [C.c_char_p]),
     "prt_profile_reset": (_I, []),
     "prt_profile_read": (_I, [_P, _I, _P, _P, _I]),
 }
 
 
-def profile_enable(on: bool) -> None:
-    lib().prt_profile_enable(1 if on else 0)
+def profile_enable(mode) -> None:
+    """0/False off, 1/True time every launch, 2 count all and time only the
+    focus kernel (profile_focus)."""
+    lib().prt_profile_enable(int(mode))
+
+
+def profile_focus(name: str) -> None:
+    lib().prt_profile_focus(name.encode())
 
 
 def profile_reset() -> None:

@@ -35,8 +35,33 @@ int cuda_status(cudaError_t e, const char *what) {
   return e == cudaErrorMemoryAllocation ? PRT_ERR_NOMEM : PRT_ERR_CUDA;
 }
 
+// The scratch comes from the device's default stream-ordered pool.  Its release
+// threshold is raised once per device so that memory freed by one call stays
+// in the pool for the next instead of going back to the driver at every
+// synchronisation (a fresh mapping of hundreds of MB per call costs more than
+// the kernels that use it).
+static void keep_pool_memory() {
+  static std::mutex mu;
+  static bool done[256] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) {
+    cudaGetLastError();
+    return;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (done[dev]) return;
+  done[dev] = true;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  cudaGetLastError();
+}
+
 int dmalloc(void **p, size_t bytes, cudaStream_t s) {
   if (bytes == 0) bytes = 16;
+  keep_pool_memory();
   cudaError_t e = cudaMallocAsync(p, bytes, s);
   if (e != cudaSuccess) {
     *p = nullptr;
@@ -298,7 +323,7 @@ __global__ void pack_leaf_kernel(const Box<T> *__restrict__ b, const int32_t *__
       leaf_perm[j] = -1;
     }
     if (j < padded) store_box(lv0, j, x);
-    if (F > 0) {
+    if constexpr (F > 0) {
       Box<T> u = x;
 #pragma unroll
       for (int o = F / 2; o > 0; o >>= 1) {
@@ -657,11 +682,14 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
   return PRT_OK;
 }
 
+// Stream-ordered release on the legacy default stream (which orders itself
+// after all blocking streams): no device-wide synchronisation.
 int prt_tree_free(prt_tree *t) {
   if (!t) return PRT_OK;
-  cudaFree(t->d_mbr);
-  cudaFree(t->d_leaf_id);
-  cudaFree(t->d_perm);
+  cudaFreeAsync(t->d_mbr, 0);
+  cudaFreeAsync(t->d_leaf_id, 0);
+  cudaFreeAsync(t->d_perm, 0);
+  cudaGetLastError();
   delete t;
   return PRT_OK;
 }

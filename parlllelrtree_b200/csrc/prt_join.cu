@@ -49,10 +49,17 @@ __global__ void __launch_bounds__(kJoinBlock) expand_kernel(JoinLevel J, const B
   constexpr int kGroups = 32 / G;
   const uint32_t gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (sub * G));
   int64_t count = J.in ? (int64_t)min((unsigned long long)J.in_cap, *J.in_count) : J.nq;
-  const int64_t warp_id = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t wb = warp_id * kGroups; wb < count; wb += n_warps * kGroups) {
-    const int64_t item = wb + sub;
+  // One output reservation per CTA iteration: the warps' hit counts are
+  // scanned in shared memory (double-buffered by iteration parity) and thread
+  // 0 does the single atomicAdd on the level counter.
+  constexpr int kWarps = kJoinBlock / 32;
+  __shared__ uint32_t s_wcount[2][kWarps];
+  __shared__ unsigned long long s_base[2];
+  const int warp = threadIdx.x >> 5;
+  const int64_t per_block = (int64_t)kWarps * kGroups;
+  int par = 0;
+  for (int64_t bb = blockIdx.x * per_block; bb < count; bb += (int64_t)gridDim.x * per_block, par ^= 1) {
+    const int64_t item = bb + warp * kGroups + sub;
     bool live = item < count;
     uint32_t q = 0, node = 0;
     if (live) {
@@ -81,12 +88,20 @@ __global__ void __launch_bounds__(kJoinBlock) expand_kernel(JoinLevel J, const B
       if (J.leaf && k) atomicAdd(reinterpret_cast<unsigned long long *>(&J.counts[3 * (int64_t)q + 2]),
                                  (unsigned long long)k);
     }
-    if (!ballot) continue;
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(J.out_count, (unsigned long long)__popc(ballot));
-    base = __shfl_sync(0xffffffffu, base, 0);
+    if (lane == 0) s_wcount[par][warp] = __popc(ballot);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t tot = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; w++) tot += s_wcount[par][w];
+      s_base[par] = tot ? atomicAdd(J.out_count, (unsigned long long)tot) : 0ull;
+    }
+    __syncthreads();
     if (hit) {
-      unsigned long long slot = base + __popc(ballot & lanemask_lt());
+      uint32_t woff = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; w++) woff += w < warp ? s_wcount[par][w] : 0u;
+      unsigned long long slot = s_base[par] + woff + __popc(ballot & lanemask_lt());
       if ((int64_t)slot < J.out_cap) {
         J.out[slot] = J.leaf ? make_uint2((uint32_t)entry, q) : make_uint2(q, (uint32_t)entry);
       }

@@ -808,14 +808,12 @@ int prt_results_area(const prt_results *r, double *d_area, void *stream) {
 
 int prt_results_free(prt_results *r) {
   if (!r) return PRT_OK;
-  cudaFree(r->pair_cstart);
-  cudaFree(r->pair_ncont);
-  cudaFree(r->status);
-  cudaFree(r->cont_vstart);
-  cudaFree(r->cont_nverts);
-  cudaFree(r->cont_hole);
-  cudaFree(r->xy);
-  cudaFree(r->pool);
+  // stream-ordered release on the legacy default stream: no device-wide sync
+  void *ptrs[] = {r->pair_cstart, r->pair_ncont, r->status, r->cont_vstart,
+                  r->cont_nverts, r->cont_hole, r->xy, r->pool};
+  for (void *p : ptrs)
+    if (p) cudaFreeAsync(p, 0);
+  cudaGetLastError();
   delete r;
   return PRT_OK;
 }

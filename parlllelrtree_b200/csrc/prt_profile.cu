@@ -13,6 +13,8 @@
 namespace prt {
 
 bool g_prof_on = false;
+static int g_prof_mode = 0;           // 1: time every launch, 2: count all, time the focus kernel only
+static std::string g_prof_focus;
 
 namespace {
 
@@ -67,6 +69,11 @@ void drain_locked() {
 
 void prof_begin(const char *name, cudaStream_t s, void **token) {
   std::lock_guard<std::mutex> lk(g_mu);
+  if (g_prof_mode == 2 && g_prof_focus != name) {
+    g_acc[name].n += 1;  // counted, not timed
+    *token = nullptr;
+    return;
+  }
   Rec *r = new Rec();
   r->name = name;
   r->a = take_event();
@@ -92,6 +99,13 @@ extern "C" {
 int prt_profile_enable(int on) {
   std::lock_guard<std::mutex> lk(g_mu);
   g_prof_on = on != 0;
+  g_prof_mode = on;
+  return PRT_OK;
+}
+
+int prt_profile_focus(const char *name) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_prof_focus = name ? name : "";
   return PRT_OK;
 }
 

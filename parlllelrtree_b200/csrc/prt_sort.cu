@@ -20,7 +20,7 @@ namespace {
 constexpr int kRadix = 256;
 constexpr int kSortBlock = 256;
 constexpr int kSortWarps = kSortBlock / 32;
-constexpr int kItems = 16;
+constexpr int kItems = 8;
 constexpr int kTile = kSortBlock * kItems;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
@@ -91,14 +91,17 @@ struct PassSmem {
   KeyT keys[kTile];
   uint32_t vals[kTile];
   uint32_t warp_hist[kSortWarps][kRadix];
+  uint32_t tile_count[kRadix];   // digit histogram of the tile (published early)
   uint32_t digit_start[kRadix];  // tile-local exclusive start of each digit
   uint32_t global_start[kRadix];
   uint32_t scan_tmp[kRadix];
   int tile;
 };
 
+constexpr int kLookBatch = 8;  // predecessor statuses read per look-back step
+
 template <typename KeyT>
-__global__ void __launch_bounds__(kSortBlock) onesweep_pass(KeyT *keys0, uint32_t *vals0, KeyT *keys1,
+__global__ void __launch_bounds__(kSortBlock, 4) onesweep_pass(KeyT *keys0, uint32_t *vals0, KeyT *keys1,
                                                            uint32_t *vals1, int64_t n, int shift,
                                                            const PassPlan *__restrict__ plan,
                                                            const uint32_t *__restrict__ goff,
@@ -114,8 +117,10 @@ __global__ void __launch_bounds__(kSortBlock) onesweep_pass(KeyT *keys0, uint32_
   uint32_t *dst_v = pp.dst ? vals1 : vals0;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int d = tid;  // kSortBlock == kRadix: thread d owns digit d
   if (tid == 0) S.tile = (int)atomicAdd(tile_ticket, 1u);
   for (int i = tid; i < kSortWarps * kRadix; i += kSortBlock) (&S.warp_hist[0][0])[i] = 0;
+  S.tile_count[d] = 0;
   __syncthreads();
   const int tile = S.tile;
   const int64_t base = (int64_t)tile * kTile;
@@ -138,64 +143,95 @@ __global__ void __launch_bounds__(kSortBlock) onesweep_pass(KeyT *keys0, uint32_
       dig[i] = kRadix + lane;  // unique: no peers, never counted
     }
   }
+  // 1. tile histogram by shared atomics, published at once so that later
+  //    tiles' look-back finds it while this tile is still ranking
+#pragma unroll
+  for (int i = 0; i < kItems; i++)
+    if (dig[i] < kRadix) atomicAdd(&S.tile_count[dig[i]], 1u);
+  __syncthreads();
+  const uint32_t total = S.tile_count[d];
+  uint32_t *st = status + (int64_t)tile * kRadix + d;
+  if (tile == 0) atomicExch(st, kFlagPrefix | ((goff[d] + total) & kCountMask));
+  else atomicExch(st, kFlagAgg | (total & kCountMask));
+
+  // 2. stable ranks: warp multisplit with __match_any_sync
   const uint32_t lt = lanemask_lt();
   uint32_t *wh = S.warp_hist[warp];
 #pragma unroll
   for (int i = 0; i < kItems; i++) {
-    uint32_t peers = __match_any_sync(0xffffffffu, dig[i]);
-    uint32_t cnt = dig[i] < kRadix ? wh[dig[i]] : 0u;
+    // lanes holding the same digit: the lowest one reads and bumps the warp's
+    // counter for it, the others get the old count by shuffle
+    const uint32_t peers = __match_any_sync(0xffffffffu, dig[i]);
+    const int leader = __ffs(peers) - 1;
+    uint32_t cnt = 0;
+    if (lane == leader && dig[i] < kRadix) {
+      cnt = wh[dig[i]];
+      wh[dig[i]] = cnt + __popc(peers);
+    }
+    cnt = __shfl_sync(0xffffffffu, cnt, leader);
     rank[i] = cnt + __popc(peers & lt);
-    __syncwarp();
-    if (dig[i] < kRadix && (peers & lt) == 0) wh[dig[i]] = cnt + __popc(peers);
-    __syncwarp();
+    __syncwarp();  // this item's counter updates before the next item's reads
   }
   __syncthreads();
-  // per digit: exclusive prefix over warps, tile total
-  const int d = tid;  // kSortBlock == kRadix
-  uint32_t total = 0;
+  // per digit: exclusive prefix over warps
+  {
+    uint32_t run = 0;
 #pragma unroll
-  for (int w = 0; w < kSortWarps; w++) {
-    uint32_t c = S.warp_hist[w][d];
-    S.warp_hist[w][d] = total;
-    total += c;
+    for (int w = 0; w < kSortWarps; w++) {
+      uint32_t c = S.warp_hist[w][d];
+      S.warp_hist[w][d] = run;
+      run += c;
+    }
   }
-  // tile-local exclusive scan over digits
-  S.scan_tmp[d] = total;
+  // tile-local exclusive scan over digits: shuffle scan per warp of 32
+  // digits, then the 8 warp totals
+  uint32_t incl = total;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) S.scan_tmp[warp] = incl;
   __syncthreads();
-  for (int o = 1; o < kRadix; o <<= 1) {
-    uint32_t t = d >= o ? S.scan_tmp[d - o] : 0u;
-    __syncthreads();
-    S.scan_tmp[d] += t;
-    __syncthreads();
-  }
-  S.digit_start[d] = S.scan_tmp[d] - total;
+  uint32_t woff = 0;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; w++) woff += w < warp ? S.scan_tmp[w] : 0u;
+  S.digit_start[d] = woff + incl - total;
 
-  // decoupled look-back for digit d
-  uint32_t *st = status + (int64_t)tile * kRadix + d;
-  uint32_t excl;
-  if (tile == 0) {
-    excl = goff[d];
-    atomicExch(st, kFlagPrefix | ((excl + total) & kCountMask));
-  } else {
-    atomicExch(st, kFlagAgg | (total & kCountMask));
+  // 3. decoupled look-back for digit d, kLookBatch predecessor statuses per
+  //    round trip; every wait is bounded
+  uint32_t excl = goff[d];
+  if (tile > 0) {
     uint32_t acc = 0;
     int t = tile - 1;
     int spins = 0;
     bool timed_out = false;
-    while (t >= 0) {
-      uint32_t s = *reinterpret_cast<volatile uint32_t *>(status + (int64_t)t * kRadix + d);
-      if ((s & ~kCountMask) == 0u) {
-        if (++spins > kSpinLimit) {
-          timed_out = true;
-          break;
-        }
-        continue;
+    for (;;) {
+      uint32_t s[kLookBatch];
+#pragma unroll
+      for (int j = 0; j < kLookBatch; j++) {
+        uint32_t sj = 2u << 30;  // before tile 0: an empty prefix (never reached)
+        if (t - j >= 0) sj = *reinterpret_cast<volatile uint32_t *>(status + (int64_t)(t - j) * kRadix + d);
+        s[j] = sj;
       }
-      acc += s & kCountMask;
-      if ((s & ~kCountMask) == kFlagPrefix) break;
-      t--;
+      int used = 0;
+      bool done = false;
+#pragma unroll
+      for (int j = 0; j < kLookBatch; j++) {
+        if (done || used < j) continue;  // stop at the first prefix or unpublished status
+        const uint32_t f = s[j] & ~kCountMask;
+        if (f == 0u) continue;           // not yet published: retry from here
+        acc += s[j] & kCountMask;
+        used = j + 1;
+        if (f == kFlagPrefix) done = true;
+      }
+      if (done) break;
+      t -= used;
+      if (used == 0 && ++spins > kSpinLimit) {
+        timed_out = true;
+        break;
+      }
     }
-    if (t < 0) acc += goff[d];  // cannot happen: tile 0 always publishes a prefix
     if (timed_out) atomicOr(err, kErrTimeout);
     excl = acc;
     atomicExch(st, kFlagPrefix | ((excl + total) & kCountMask));
@@ -203,7 +239,7 @@ __global__ void __launch_bounds__(kSortBlock) onesweep_pass(KeyT *keys0, uint32_
   S.global_start[d] = excl;
   __syncthreads();
 
-  // stage in digit order
+  // 4. stage in digit order, then write out in coalesced runs
 #pragma unroll
   for (int i = 0; i < kItems; i++) {
     if (dig[i] < kRadix) {

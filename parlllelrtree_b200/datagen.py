@@ -31,13 +31,21 @@ __all__ = [
     "quantise",
     "layer_bboxes",
     "layer_from_rings",
+    "star_layer_device",
+    "mixture_means",
 ]
 
 
+def mixture_means(k: int = 64, seed: int = 0) -> np.ndarray:
+    """The mixture's ``k`` means, uniform in the unit square; one fixed set
+    (seed 0) shared by every layer and box set so that layers overlap."""
+    return np.random.default_rng(10_000 + seed).random((k, 2))
+
+
 def mixture_centres(rng: np.random.Generator, n: int, k: int = 64, sigma: float = 0.02) -> np.ndarray:
-    """``n`` points from a mixture of ``k`` isotropic Gaussians with means
-    uniform in the unit square, clipped to the square."""
-    means = rng.random((k, 2))
+    """``n`` points from a mixture of ``k`` isotropic Gaussians (the fixed
+    means of ``mixture_means``), clipped to the unit square."""
+    means = mixture_means(k)
     comp = rng.integers(0, k, size=n)
     pts = means[comp] + rng.normal(0.0, sigma, size=(n, 2))
     np.clip(pts, 0.0, 1.0, out=pts)
@@ -81,8 +89,20 @@ def quantise(boxes: np.ndarray, scale: float = 1e6) -> np.ndarray:
     return np.rint(np.asarray(boxes, dtype=np.float64) * scale).astype(np.int64)
 
 
+def _lobe_weight(nv):
+    """Weight of the smooth radial profile: 0 up to 32 vertices (radii
+    r * U(0.5, 1) per vertex, the small star configuration), growing towards 1
+    for large rings, whose radius then follows a few smooth lobes plus a small
+    per-vertex jitter.  Independent per-vertex jitter on thousands of vertices
+    would give spiky rings that every scanline crosses hundreds of times."""
+    nv = np.asarray(nv, dtype=np.float64)
+    return np.clip((nv - 32.0) / np.maximum(nv, 1.0), 0.0, 1.0)
+
+
 def _star_rings(rng, centres, radii, nverts):
-    """CCW star rings: jittered sorted angles, radii r * U(0.5, 1)."""
+    """CCW star rings: jittered sorted angles; radius r * ((1 - w) U(0.5, 1)
+    + w (0.75 + 0.25 L(theta))) with L a sum of 5 random sine lobes scaled to
+    [-1, 1] and w = _lobe_weight(n), so every vertex lies between 0.5 r and r."""
     nv = np.asarray(nverts, dtype=np.int64)
     total = int(nv.sum())
     ring_vert = np.zeros(len(nv) + 1, dtype=np.int64)
@@ -92,7 +112,15 @@ def _star_rings(rng, centres, radii, nverts):
     step = 2.0 * np.pi / nv[owner]
     # jitter inside each vertex's own angular slot keeps the angles sorted
     theta = (k + 0.1 + 0.8 * rng.random(total)) * step
-    rad = radii[owner] * rng.uniform(0.5, 1.0, size=total)
+    jit = rng.uniform(0.5, 1.0, size=total)
+    amp = rng.random((len(nv), 5))
+    amp /= amp.sum(axis=1, keepdims=True)
+    phase = rng.uniform(0.0, 2.0 * np.pi, size=(len(nv), 5))
+    lobe = np.zeros(total)
+    for m in range(5):
+        lobe += amp[owner, m] * np.sin((m + 1) * theta + phase[owner, m])
+    w = _lobe_weight(nv)[owner]
+    rad = radii[owner] * ((1.0 - w) * jit + w * (0.75 + 0.25 * lobe))
     xy = np.empty((total, 2), dtype=np.float64)
     xy[:, 0] = centres[owner, 0] + rad * np.cos(theta)
     xy[:, 1] = centres[owner, 1] + rad * np.sin(theta)
@@ -131,25 +159,67 @@ def star_layer(n: int, seed: int, nv_lo: int = 8, nv_hi: int = 32,
             "xy": outer_xy,
         }
     has_holes = rng.random(n) < hole_frac
-    nholes = np.where(has_holes, rng.integers(1, 4, size=n), 0)
-    rings, holes = [], []
-    for p in range(n):
-        rings.append(outer_xy[outer_vert[p]:outer_vert[p + 1]])
-        holes.append(0)
-        h = int(nholes[p])
-        for j in range(h):
-            # hole j sits in its own angular sector of the inner disk
-            a0 = 2.0 * np.pi * j / h
-            span = 2.0 * np.pi / h
-            m = int(rng.integers(3, 5))
-            ang = a0 + span * (0.15 + 0.7 * np.sort(rng.random(m)))[::-1]  # CW
-            rr = radii[p] * rng.uniform(0.15, 0.45, size=m)
-            ring = np.stack([centre_xy[p, 0] + rr * np.cos(ang),
-                             centre_xy[p, 1] + rr * np.sin(ang)], axis=1)
-            rings.append(ring)
-            holes.append(1)
-    counts = [1 + int(nholes[p]) for p in range(n)]
-    return layer_from_rings(rings, holes, counts)
+    nholes = np.where(has_holes, rng.integers(1, 4, size=n), 0).astype(np.int64)
+    return _with_holes(rng, outer_vert, outer_xy, nverts, nholes, centre_xy, radii)
+
+
+def _with_holes(rng, outer_vert, outer_xy, nverts, nholes, centre_xy, radii) -> dict:
+    """Interleaves 1-3 clockwise hole rings (3-4 vertices each) after each
+    polygon's outer ring.  Hole j of h sits in its own angular sector, at radii
+    below the star's guaranteed inner radius: consecutive outer vertices are
+    at radius >= 0.5 r and at most 1.8 * 2 pi / n apart in angle, so the outer
+    boundary stays beyond 0.5 r cos(1.8 pi / n)."""
+    n = len(nverts)
+    rings_per_poly = 1 + nholes
+    poly_ring = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(rings_per_poly, out=poly_ring[1:])
+    n_rings = int(poly_ring[-1])
+    ring_poly = np.repeat(np.arange(n), rings_per_poly)
+    ring_j = np.arange(n_rings) - poly_ring[ring_poly]          # 0 = outer, k >= 1 = hole k-1
+    is_hole = ring_j > 0
+    hole_m = rng.integers(3, 5, size=n_rings)                   # vertices of each hole ring
+    ring_nv = np.where(is_hole, hole_m, nverts[ring_poly])
+    ring_vert = np.zeros(n_rings + 1, dtype=np.int64)
+    np.cumsum(ring_nv, out=ring_vert[1:])
+    xy = np.empty((int(ring_vert[-1]), 2), dtype=np.float64)
+    # outer rings: move each polygon's block of vertices to its ring's slot
+    outer_ring = poly_ring[:-1]
+    owner = np.repeat(np.arange(n), nverts)
+    k = np.arange(len(outer_xy)) - outer_vert[owner]
+    xy[ring_vert[outer_ring][owner] + k] = outer_xy
+    # hole rings
+    hr = np.nonzero(is_hole)[0]
+    if len(hr):
+        hp = ring_poly[hr]
+        h = nholes[hp]
+        j = ring_j[hr] - 1
+        m = ring_nv[hr]
+        hv_owner = np.repeat(np.arange(len(hr)), m)
+        hk = np.arange(int(m.sum())) - np.repeat(np.cumsum(m) - m, m)
+        # each hole spans at most 0.9 pi of its sector, so no two consecutive
+        # hole vertices are more than pi apart in angle (a simple CW ring)
+        sector = 2.0 * np.pi / h[hv_owner]
+        span = np.minimum(sector, 0.9 * np.pi)
+        a0 = sector * j[hv_owner] + 0.5 * (sector - span)
+        # angles inside the sector, descending within each ring (clockwise):
+        # sort by (ring, -value); rings occupy contiguous slots, so the sorted
+        # values land on their own ring's vertices
+        raw = rng.random(len(hk))
+        frac = raw[np.lexsort((-raw, hv_owner))]
+        ang = a0 + span * (0.15 + 0.7 * frac)
+        nv_out = nverts[hp][hv_owner]
+        rin = 0.5 * np.cos(np.minimum(1.8 * np.pi / np.maximum(nv_out, 4), 1.45))
+        # one radius per hole: its vertices lie on a circle arc in descending
+        # angle, a convex clockwise ring
+        rr = (radii[hp] * rng.uniform(0.3, 0.9, size=len(hr)))[hv_owner] * rin
+        xy[ring_vert[hr][hv_owner] + hk, 0] = centre_xy[hp][hv_owner, 0] + rr * np.cos(ang)
+        xy[ring_vert[hr][hv_owner] + hk, 1] = centre_xy[hp][hv_owner, 1] + rr * np.sin(ang)
+    return {
+        "poly_ring": poly_ring,
+        "ring_vert": ring_vert,
+        "ring_hole": is_hole.astype(np.int32),
+        "xy": xy,
+    }
 
 
 def layer_from_rings(rings, holes, rings_per_poly) -> dict:
@@ -181,3 +251,76 @@ def layer_bboxes(layer: dict) -> np.ndarray:
     out[:, 3] = np.maximum.reduceat(xy[:, 1], vstart)
     assert np.all(vend > vstart)
     return out
+
+
+def star_layer_device(n: int, seed: int, nv_lo: int = 4, nv_hi: int = 4096, r_lo: float = 1e-3,
+                      r_hi: float = 1e-2, zipf: float | None = 1.2, hole_frac: float = 0.05,
+                      centres: str = "mixture", device: str = "cuda") -> dict:
+    """``star_layer`` for large layers: the per-polygon draws (vertex counts,
+    radii, centres, holes) come from numpy exactly as in ``star_layer``, the
+    per-vertex draws and trigonometry run in torch on ``device``.  Returns the
+    same dict with torch tensors on the device.  Same distribution as
+    ``star_layer``, not the same numbers."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    if zipf is not None:
+        nverts = np.clip(rng.zipf(zipf, size=n), nv_lo, nv_hi).astype(np.int64)
+    else:
+        nverts = rng.integers(nv_lo, nv_hi + 1, size=n).astype(np.int64)
+    radii = np.exp(rng.uniform(np.log(r_lo), np.log(r_hi), size=n))
+    centre_xy = mixture_centres(rng, n) if centres == "mixture" else rng.random((n, 2))
+    has_holes = rng.random(n) < hole_frac
+    nholes = np.where(has_holes, rng.integers(1, 4, size=n), 0).astype(np.int64)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    dev = torch.device(device)
+    nv = torch.from_numpy(nverts).to(dev)
+    rad = torch.from_numpy(radii).to(dev)
+    cen = torch.from_numpy(centre_xy).to(dev)
+    # rings: outer ring of polygon p, then its holes
+    rings_per_poly = torch.from_numpy(1 + nholes).to(dev)
+    poly_ring = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    torch.cumsum(rings_per_poly, 0, out=poly_ring[1:])
+    n_rings = int(poly_ring[-1])
+    ring_poly = torch.repeat_interleave(torch.arange(n, device=dev), rings_per_poly)
+    ring_j = torch.arange(n_rings, device=dev) - poly_ring[ring_poly]
+    is_hole = ring_j > 0
+    hole_m = torch.randint(3, 5, (n_rings,), generator=g, device=dev)
+    ring_nv = torch.where(is_hole, hole_m, nv[ring_poly])
+    ring_vert = torch.zeros(n_rings + 1, dtype=torch.int64, device=dev)
+    torch.cumsum(ring_nv, 0, out=ring_vert[1:])
+    total = int(ring_vert[-1])
+    owner_ring = torch.repeat_interleave(torch.arange(n_rings, device=dev), ring_nv)
+    k = torch.arange(total, device=dev) - ring_vert[owner_ring]
+    p = ring_poly[owner_ring]
+    hole_v = is_hole[owner_ring]
+    u = torch.rand(total, generator=g, device=dev, dtype=torch.float64)
+    # outer rings: jittered angle slots, radius r * U(0.5, 1), CCW
+    step = 2.0 * np.pi / nv[p].to(torch.float64)
+    theta = (k.to(torch.float64) + 0.1 + 0.8 * u) * step
+    jit = 0.5 + 0.5 * torch.rand(total, generator=g, device=dev, dtype=torch.float64)
+    amp = torch.from_numpy(rng.random((n, 5))).to(dev)
+    amp = amp / amp.sum(dim=1, keepdim=True)
+    phase = torch.from_numpy(rng.uniform(0.0, 2.0 * np.pi, size=(n, 5))).to(dev)
+    lobe = torch.zeros(total, dtype=torch.float64, device=dev)
+    for mm in range(5):
+        lobe += amp[p, mm] * torch.sin((mm + 1) * theta + phase[p, mm])
+    w = torch.from_numpy(_lobe_weight(nverts)).to(dev)[p]
+    rr = rad[p] * ((1.0 - w) * jit + w * (0.75 + 0.25 * lobe))
+    # holes: on a circle arc of their sector, descending angle (CW)
+    h = torch.from_numpy(nholes).to(dev)[p].clamp(min=1).to(torch.float64)
+    sector = 2.0 * np.pi / h
+    span = torch.clamp(sector, max=0.9 * np.pi)
+    a0 = sector * (ring_j[owner_ring] - 1).clamp(min=0).to(torch.float64) + 0.5 * (sector - span)
+    m = ring_nv[owner_ring].to(torch.float64)
+    frac = (m - 1 - k.to(torch.float64) + 0.5) / m  # evenly spaced, descending
+    hang = a0 + span * (0.15 + 0.7 * frac)
+    rin = 0.5 * torch.cos(torch.clamp(1.8 * np.pi / nv[p].clamp(min=4).to(torch.float64), max=1.45))
+    hr = (rad * torch.from_numpy(rng.uniform(0.3, 0.9, size=n)).to(dev))[p] * rin
+    ang = torch.where(hole_v, hang, theta)
+    r_all = torch.where(hole_v, hr, rr)
+    xy = torch.empty((total, 2), dtype=torch.float64, device=dev)
+    xy[:, 0] = cen[p, 0] + r_all * torch.cos(ang)
+    xy[:, 1] = cen[p, 1] + r_all * torch.sin(ang)
+    return {"poly_ring": poly_ring, "ring_vert": ring_vert, "ring_hole": is_hole.to(torch.int32), "xy": xy}
