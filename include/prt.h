@@ -233,6 +233,75 @@ int prt_clip_pair_host(int op, int s_ncont, const int32_t *s_nverts, const doubl
                        int32_t *out_ncont, int32_t cont_cap, int32_t *out_nverts,
                        int32_t *out_hole, int64_t *out_nv, int64_t vert_cap, double *out_xy);
 
+/* ---------------------------------------------------------------- graph pipeline */
+
+/* The whole overlay (the caller the reference leaves out around
+ * vector_map_overlay_gpc_kernel.cu:61-113): polygon MBRs of both layers ->
+ * bottom-up Morton R-tree over the base layer -> breadth-first join of the
+ * overlay layer's MBRs -> batched clip of every candidate pair.  All buffers
+ * are allocated by prt_pipeline_create for the capacities in the config; the
+ * first prt_pipeline_run captures the launches into a CUDA graph and every run
+ * replays it (one cudaGraphLaunch, no host synchronisation).  The layers are
+ * referenced, not copied: their vertex coordinates may change between runs
+ * (the counts may not).  No reference counterpart (a new entry point). */
+/* ---------------------------------------------------------------- batched schedule */
+
+/* How the batched schedule (PRT_SCHED_BATCHED and the graph pipeline) cuts
+ * the size-sorted pairs into bins and clips them (no reference counterpart;
+ * the reference runs one pair per thread in input order).  Bin b holds the
+ * pairs whose vertex count n_subject + n_clip lies in
+ * (bin_thresholds[b+1], bin_thresholds[b]]; bins are clipped largest first
+ * in one persistent launch.  bin_warp_mode[b] = 1 clips each pair of the bin
+ * with a whole warp (active edge table in shared memory, aet_slots slots per
+ * warp; pairs whose table outgrows it are clipped by one thread), 0 with one
+ * thread per pair.  bin_warps_per_sm[b] persistent warps per SM start on bin b
+ * and steal from the smaller bins once theirs is empty. */
+#define PRT_MAX_BINS 8
+typedef struct {
+  int32_t nbins;
+  int32_t aet_slots;
+  int64_t bin_thresholds[PRT_MAX_BINS];
+  int32_t bin_warp_mode[PRT_MAX_BINS];
+  int32_t bin_warps_per_sm[PRT_MAX_BINS];
+} prt_schedule;
+
+/* Sets the schedule used by later calls of this process (NULL restores the
+ * built-in default); returns PRT_ERR_INVALID for an inconsistent one. */
+int prt_schedule_set(const prt_schedule *sched);
+int prt_schedule_get(prt_schedule *sched);
+
+typedef struct {
+  int32_t fanout;             /* tree fanout (default 16) */
+  int32_t op;                 /* PRT_GPC_* (default PRT_GPC_INT when cfg is NULL) */
+  int64_t max_pairs;          /* candidate pairs kept (default 8 x max layer size) */
+  int64_t max_frontier;       /* join frontier items per level (default 64 x overlay + 1 Mi) */
+  int64_t max_out_contours;   /* result pool sizes (defaults from the pair and vertex counts) */
+  int64_t max_out_vertices;
+  int64_t arena_budget_bytes; /* clip scratch (default a third of free memory, at most 48 GB) */
+  const prt_schedule *sched;  /* NULL: the schedule set by prt_schedule_set */
+} prt_pipeline_config;
+
+typedef struct prt_pipeline prt_pipeline;
+
+int prt_pipeline_create(const prt_layer *base, const prt_layer *overlay, const prt_pipeline_config *cfg,
+                        prt_pipeline **out);
+/* Enqueues one run on `stream` (a non-default stream). */
+int prt_pipeline_run(prt_pipeline *p, void *stream);
+/* Synchronises, then: sizes[0] candidate pairs found, [1] contours,
+ * [2] vertices, [3] non-empty results, [4] pairs that did not fit their
+ * arena or the result pools (their results are empty; rerun with larger
+ * capacities), [5] largest join frontier, [6] 1 when pairs or frontier
+ * exceeded their capacity, [7] 1 when a bounded wait timed out. */
+int prt_pipeline_sizes(prt_pipeline *p, int64_t *sizes);
+/* Copies the first min(cap, pairs found) candidate pairs {nodeid, queryid}
+ * and the leaf order (record id per leaf entry, one per base polygon) of the
+ * last run into caller buffers, host or device (either may be NULL). */
+int prt_pipeline_pairs(prt_pipeline *p, prt_pair *pairs, int64_t cap, int32_t *leaf_to_poly);
+/* Results of the last run in pair order, as prt_results_copy. */
+int prt_pipeline_results(prt_pipeline *p, int64_t *h_pair_cont_off, int32_t *h_cont_nverts,
+                         int32_t *h_cont_hole, double *h_xy);
+int prt_pipeline_free(prt_pipeline *p);
+
 /* ---------------------------------------------------------------- area + adjoint */
 
 /* Intersection area of each pair (subject = base polygon pair_a[i], clip =

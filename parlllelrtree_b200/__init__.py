@@ -29,7 +29,8 @@ from ._lib import COORD, KEY, OP, SCHED, PrtError, check, lib
 
 __all__ = [
     "Tree", "Layer", "Results", "build_bottomup", "build_topdown", "overlay", "overlay_ref", "clip_pair",
-    "intersection_area", "IntersectionArea", "PrtError", "device_count",
+    "intersection_area", "IntersectionArea", "PrtError", "device_count", "Pipeline", "get_schedule",
+    "set_schedule", "schedule",
 ]
 
 _DT2COORD = {torch.int64: COORD["i64"], torch.float32: COORD["f32"], torch.float64: COORD["f64"],
@@ -280,6 +281,134 @@ def overlay(pairs, base: Layer, over: Layer, leaf_to_poly=None, offset: int = 0,
     check(lib().prt_overlay_run(_ptr(p), len(p), offset, _ptr(l2p), C.byref(sb), C.byref(so), OP[op], SCHED[sched],
                                 _stream(), C.byref(h)))
     return Results(h)
+
+
+MAX_BINS = 8
+
+
+class _Schedule(C.Structure):
+    _fields_ = [("nbins", C.c_int32), ("aet_slots", C.c_int32), ("bin_thresholds", C.c_int64 * MAX_BINS),
+                ("bin_warp_mode", C.c_int32 * MAX_BINS), ("bin_warps_per_sm", C.c_int32 * MAX_BINS)]
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "_Schedule":
+        s = cls()
+        thr = list(d["thresholds"])
+        s.nbins = len(thr)
+        s.aet_slots = int(d.get("aet_slots", 256))
+        wm = list(d.get("warp_mode", [0] * len(thr)))
+        wps = list(d.get("warps_per_sm", [4] * len(thr)))
+        for b in range(len(thr)):
+            s.bin_thresholds[b] = int(thr[b])
+            s.bin_warp_mode[b] = int(wm[b])
+            s.bin_warps_per_sm[b] = int(wps[b])
+        return s
+
+    def to_dict(self) -> dict:
+        n = self.nbins
+        return {"thresholds": [int(self.bin_thresholds[b]) for b in range(n)],
+                "warp_mode": [int(self.bin_warp_mode[b]) for b in range(n)],
+                "warps_per_sm": [int(self.bin_warps_per_sm[b]) for b in range(n)],
+                "aet_slots": int(self.aet_slots)}
+
+
+def get_schedule() -> dict:
+    """The batched schedule in use (prt_schedule_get): size-bin thresholds
+    (descending vertex-count upper bounds), per-bin warp mode (1 = one pair
+    per warp) and persistent warps per SM, and the warp clipper's AET slots."""
+    s = _Schedule()
+    check(lib().prt_schedule_get(C.byref(s)))
+    return s.to_dict()
+
+
+def set_schedule(sched: dict | None) -> None:
+    """Sets the batched schedule for later calls (None = built-in default)."""
+    if sched is None:
+        check(lib().prt_schedule_set(None))
+    else:
+        check(lib().prt_schedule_set(C.byref(_Schedule.from_dict(sched))))
+
+
+class schedule:
+    """Context manager: ``with prt.schedule(d): ...`` runs with schedule ``d``."""
+
+    def __init__(self, sched: dict | None):
+        self.sched = sched
+
+    def __enter__(self):
+        self.prev = get_schedule()
+        set_schedule(self.sched)
+        return self
+
+    def __exit__(self, *exc):
+        set_schedule(self.prev)
+        return False
+
+
+class _PipelineConfig(C.Structure):
+    _fields_ = [("fanout", C.c_int32), ("op", C.c_int32), ("max_pairs", C.c_int64), ("max_frontier", C.c_int64),
+                ("max_out_contours", C.c_int64), ("max_out_vertices", C.c_int64),
+                ("arena_budget_bytes", C.c_int64), ("sched", C.c_void_p)]
+
+
+class Pipeline:
+    """The build -> join -> clip overlay captured as one CUDA graph
+    (prt_pipeline_*): tree over ``base``'s polygon MBRs, join of ``over``'s,
+    batched clip of every candidate pair.  ``run()`` replays the graph on the
+    current stream (which must not be the legacy default stream)."""
+
+    def __init__(self, base: Layer, over: Layer, fanout: int = 16, op: str = "int", max_pairs: int = 0,
+                 max_frontier: int = 0, max_out_contours: int = 0, max_out_vertices: int = 0,
+                 arena_budget_bytes: int = 0, sched: dict | None = None):
+        self.base, self.over = base, over  # the graph reads their buffers
+        cfg = _PipelineConfig()
+        cfg.fanout, cfg.op = fanout, OP[op]
+        cfg.max_pairs, cfg.max_frontier = max_pairs, max_frontier
+        cfg.max_out_contours, cfg.max_out_vertices = max_out_contours, max_out_vertices
+        cfg.arena_budget_bytes = arena_budget_bytes
+        self._sched = _Schedule.from_dict(sched) if sched is not None else None
+        cfg.sched = C.addressof(self._sched) if self._sched is not None else None
+        self._sb, self._so = base.struct(), over.struct()
+        self._h = C.c_void_p()
+        check(lib().prt_pipeline_create(C.byref(self._sb), C.byref(self._so), C.byref(cfg), C.byref(self._h)))
+        self._max_pairs = max_pairs if max_pairs > 0 else 8 * max(base.n_poly, over.n_poly)
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().prt_pipeline_free(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    def run(self) -> None:
+        check(lib().prt_pipeline_run(self._h, _stream()))
+
+    def sizes(self) -> dict:
+        s = np.zeros(8, dtype=np.int64)
+        check(lib().prt_pipeline_sizes(self._h, s.ctypes.data_as(C.c_void_p)))
+        keys = ("pairs", "contours", "vertices", "nonempty", "failed", "max_frontier", "overflow", "timeout")
+        return dict(zip(keys, (int(x) for x in s)))
+
+    def pairs(self):
+        """(pairs int32 [n, 2] {nodeid, queryid}, leaf_to_poly int32 [P]) of the last run, on the device."""
+        n = min(self.sizes()["pairs"], self._max_pairs)
+        pairs = torch.empty((max(n, 1), 2), dtype=torch.int32, device="cuda")
+        l2p = torch.empty(self.base.n_poly, dtype=torch.int32, device="cuda")
+        check(lib().prt_pipeline_pairs(self._h, _ptr(pairs), n, _ptr(l2p)))
+        return pairs[:n], l2p
+
+    def to_host(self):
+        """(pair_cont_off, cont_nverts, cont_hole, xy) in pair order, as Results.to_host."""
+        s = self.sizes()
+        n = s["pairs"]
+        off = np.zeros(n + 1, np.int64)
+        nv = np.zeros(max(s["contours"], 1), np.int32)
+        hole = np.zeros(max(s["contours"], 1), np.int32)
+        xy = np.zeros((max(s["vertices"], 1), 2), np.float64)
+        p = lambda a: a.ctypes.data_as(C.c_void_p)
+        check(lib().prt_pipeline_results(self._h, p(off), p(nv), p(hole), p(xy)))
+        return off, nv[: s["contours"]], hole[: s["contours"]], xy
 
 
 def overlay_ref(pairs, num_base, prefix_base, vertex_base, hole_base, num_over, prefix_over, vertex_over, hole_over,

@@ -53,6 +53,14 @@ _SIGS = {
     "prt_results_area": (_I, [_P, _P, _P]),
     "prt_results_free": (_I, [_P]),
     "prt_clip_pair_host": (_I, [_I, _I, _P, _P, _I, _P, _P, _P, C.c_int32, _P, _P, _P, _I64, _P]),
+    "prt_schedule_set": (_I, [_P]),
+    "prt_schedule_get": (_I, [_P]),
+    "prt_pipeline_create": (_I, [_P, _P, _P, _P]),
+    "prt_pipeline_run": (_I, [_P, _P]),
+    "prt_pipeline_sizes": (_I, [_P, _P]),
+    "prt_pipeline_pairs": (_I, [_P, _P, _I64, _P]),
+    "prt_pipeline_results": (_I, [_P, _P, _P, _P, _P]),
+    "prt_pipeline_free": (_I, [_P]),
     "prt_area_fwd": (_I, [_P, _P, _I64, _P, _P, _P, _P]),
     "prt_area_bwd": (_I, [_P, _P, _I64, _P, _P, _P, _P, _P, _P]),
     "prt_profile_enable": (_I, [_I]),

@@ -463,59 +463,34 @@ int finish(unsigned *d_err, cudaStream_t s, int rc) {
 }
 
 }  // namespace
-}  // namespace prt
 
-using namespace prt;
-
-extern "C" {
-
-const char *prt_last_error(void) { return g_err.c_str(); }
-int prt_version(void) { return 1; }
-
-int prt_device_count(void) {
-  int n = 0;
-  if (cudaGetDeviceCount(&n) != cudaSuccess) {
-    cudaGetLastError();
-    return 0;
-  }
-  return n;
-}
-
-int prt_build_bottomup(const void *d_boxes, int coord_type, const int32_t *d_ids, int64_t n, int fanout,
-                       int key_mode, void *stream, prt_tree **out) {
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  PRT_CHECK(key_mode == PRT_KEY_MORTON32 || key_mode == PRT_KEY_REF64, PRT_ERR_INVALID, "key mode %d",
-            key_mode);
-  PRT_CHECK(key_mode != PRT_KEY_REF64 || coord_type == PRT_COORD_I64, PRT_ERR_INVALID,
-            "REF64 keys need int64 boxes");
-  prt_tree *t = nullptr;
-  int rc = new_tree(d_boxes, coord_type, n, fanout, PRT_BOTTOM_UP, key_mode, s, &t);
-  if (rc) return rc;
+// Enqueues the bottom-up build of `t` (allocated by tree_alloc) from d_boxes
+// without any host synchronisation, so it can be captured in a CUDA graph;
+// *d_err (device, zeroed by the caller) receives kErrTimeout if a sort
+// look-back wait gives up.
+int bu_enqueue(prt_tree *t, const void *d_boxes, const int32_t *d_ids, unsigned *err, cudaStream_t s) {
+  const int64_t n = t->n;
   // scratch: ext (4 x 8), err, sel, keys0/1, vals0/1
   unsigned char *scr = nullptr;
-  size_t kb = key_mode == PRT_KEY_REF64 ? 8 : 4;
+  size_t kb = t->key_mode == PRT_KEY_REF64 ? 8 : 4;
   size_t need = 64 + 2 * kb * n + 2 * 4 * n + 64;
-  rc = dmalloc(reinterpret_cast<void **>(&scr), need, s);
-  if (rc) {
-    prt_tree_free(t);
-    return rc;
-  }
+  int rc = dmalloc(reinterpret_cast<void **>(&scr), need, s);
+  if (rc) return rc;
   unsigned long long *ext = reinterpret_cast<unsigned long long *>(scr);
-  unsigned *err = reinterpret_cast<unsigned *>(scr + 32);
   int *sel = reinterpret_cast<int *>(scr + 36);
   unsigned char *kp = scr + 64;
   void *keys0 = kp, *keys1 = kp + kb * n;
   uint32_t *vals0 = reinterpret_cast<uint32_t *>(kp + 2 * kb * n);
   uint32_t *vals1 = vals0 + n;
-  cudaError_t e = cudaMemsetAsync(err, 0, 8, s);
+  cudaError_t e = cudaSuccess;
   int g = grid_for(n, 256, 16);
   if (e == cudaSuccess) {
-    if (key_mode == PRT_KEY_MORTON32) {
+    if (t->key_mode == PRT_KEY_MORTON32) {
       {
         PRT_PROF("extent_init", s);
         extent_init_kernel<<<1, 1, 0, s>>>(ext);
       }
-      rc = dispatch_coord(coord_type, [&](auto tag) {
+      rc = dispatch_coord(t->coord, [&](auto tag) {
         using T = decltype(tag);
         const Box<T> *b = reinterpret_cast<const Box<T> *>(d_boxes);
         {
@@ -552,12 +527,56 @@ int prt_build_bottomup(const void *d_boxes, int coord_type, const int32_t *d_ids
   } else {
     rc = cuda_status(e, "memset");
   }
-  if (!rc) rc = dispatch_coord(coord_type, [&](auto tag) {
+  if (!rc) rc = dispatch_coord(t->coord, [&](auto tag) {
     using T = decltype(tag);
     return pack_tree<T>(t, d_boxes, d_ids, vals0, vals1, sel, s);
   });
-  rc = finish(err, s, rc);
   dfree(scr, s);
+  return rc;
+}
+
+int tree_alloc(const void *d_boxes, int coord, int64_t n, int fanout, int kind, int key_mode, cudaStream_t s,
+               prt_tree **out) {
+  return new_tree(d_boxes, coord, n, fanout, kind, key_mode, s, out);
+}
+
+}  // namespace prt
+
+using namespace prt;
+
+extern "C" {
+
+const char *prt_last_error(void) { return g_err.c_str(); }
+int prt_version(void) { return 1; }
+
+int prt_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int prt_build_bottomup(const void *d_boxes, int coord_type, const int32_t *d_ids, int64_t n, int fanout,
+                       int key_mode, void *stream, prt_tree **out) {
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  PRT_CHECK(key_mode == PRT_KEY_MORTON32 || key_mode == PRT_KEY_REF64, PRT_ERR_INVALID, "key mode %d",
+            key_mode);
+  PRT_CHECK(key_mode != PRT_KEY_REF64 || coord_type == PRT_COORD_I64, PRT_ERR_INVALID,
+            "REF64 keys need int64 boxes");
+  prt_tree *t = nullptr;
+  int rc = new_tree(d_boxes, coord_type, n, fanout, PRT_BOTTOM_UP, key_mode, s, &t);
+  if (rc) return rc;
+  unsigned *err = nullptr;
+  rc = dalloc(&err, 2, s);
+  if (!rc) {
+    cudaError_t e = cudaMemsetAsync(err, 0, 8, s);
+    if (e != cudaSuccess) rc = cuda_status(e, "memset");
+  }
+  if (!rc) rc = bu_enqueue(t, d_boxes, d_ids, err, s);
+  rc = finish(err, s, rc);
+  dfree(err, s);
   if (rc) {
     prt_tree_free(t);
     return rc;

@@ -498,12 +498,167 @@ __device__ inline void build_intersection_table(Arena &A, int &it, int aet, doub
   }
 }
 
+// Intersections of one scanbeam (GPC:461-659): builds the intersection table
+// of the AET for beam height dy, then processes each intersection in y order:
+// output vertices at the crossing and the swap of the two bundles in the AET.
+// Shared by the thread and the warp clippers.
+__device__ inline void intersect_beam(Arena &A, int op, int &aet, int &out_poly, double yb, double dy) {
+  Edge *E = A.E;
+  int it = -1;
+  int in[2];
+  build_intersection_table(A, it, aet, dy);
+  if (A.status) return;
+  int g4 = 0;
+  for (int in_ = it; in_ >= 0 && !A.status; in_ = A.IT[in_].next) {
+    PRT_GUARD(g4, A.nit)
+    const int a0 = A.IT[in_].e0, a1 = A.IT[in_].e1;
+    Edge &x0 = E[a0];
+    Edge &x1 = E[a1];
+    if ((x0.bundle[ABOVE][CLIP] || x0.bundle[ABOVE][SUBJ]) && (x1.bundle[ABOVE][CLIP] || x1.bundle[ABOVE][SUBJ])) {
+      const int p = x0.outp[ABOVE], q = x1.outp[ABOVE];
+      const double ix = A.IT[in_].x;
+      const double iy = A.IT[in_].y + yb;
+      const int b0C = x0.bundle[ABOVE][CLIP], b0S = x0.bundle[ABOVE][SUBJ];
+      const int b1C = x1.bundle[ABOVE][CLIP], b1S = x1.bundle[ABOVE][SUBJ];
+      in[CLIP] = (b0C && !x0.bside[CLIP]) || (b1C && x1.bside[CLIP]) ||
+                 (!b0C && !b1C && x0.bside[CLIP] && x1.bside[CLIP]);
+      in[SUBJ] = (b0S && !x0.bside[SUBJ]) || (b1S && x1.bside[SUBJ]) ||
+                 (!b0S && !b1S && x0.bside[SUBJ] && x1.bside[SUBJ]);
+      int tr = 0, tl = 0, br = 0, bl = 0;
+      switch (op) {
+        case OP_DIFF:
+        case OP_INT:
+          tr = in[CLIP] && in[SUBJ];
+          tl = (in[CLIP] ^ b1C) && (in[SUBJ] ^ b1S);
+          br = (in[CLIP] ^ b0C) && (in[SUBJ] ^ b0S);
+          bl = (in[CLIP] ^ b1C ^ b0C) && (in[SUBJ] ^ b1S ^ b0S);
+          break;
+        case OP_XOR:
+          tr = in[CLIP] ^ in[SUBJ];
+          tl = (in[CLIP] ^ b1C) ^ (in[SUBJ] ^ b1S);
+          br = (in[CLIP] ^ b0C) ^ (in[SUBJ] ^ b0S);
+          bl = (in[CLIP] ^ b1C ^ b0C) ^ (in[SUBJ] ^ b1S ^ b0S);
+          break;
+        default:
+          tr = in[CLIP] || in[SUBJ];
+          tl = (in[CLIP] ^ b1C) || (in[SUBJ] ^ b1S);
+          br = (in[CLIP] ^ b0C) || (in[SUBJ] ^ b0S);
+          bl = (in[CLIP] ^ b1C ^ b0C) || (in[SUBJ] ^ b1S ^ b0S);
+          break;
+      }
+      const int vclass = tr + (tl << 1) + (br << 2) + (bl << 3);
+      switch (vclass) {
+        case EMN:
+        case IMN:
+          add_local_min(A, out_poly, a0, ix, iy);
+          x1.outp[ABOVE] = x0.outp[ABOVE];
+          break;
+        case ERI:
+          if (p >= 0) {
+            add_right(A, p, ix, iy);
+            x1.outp[ABOVE] = p;
+            x0.outp[ABOVE] = -1;
+          }
+          break;
+        case ELI:
+          if (q >= 0) {
+            add_left(A, q, ix, iy);
+            x0.outp[ABOVE] = q;
+            x1.outp[ABOVE] = -1;
+          }
+          break;
+        case EMX:
+          if (p >= 0 && q >= 0) {
+            add_left(A, p, ix, iy);
+            merge_right(A, p, q, out_poly);
+            x0.outp[ABOVE] = -1;
+            x1.outp[ABOVE] = -1;
+          }
+          break;
+        case ILI:
+          if (p >= 0) {
+            add_left(A, p, ix, iy);
+            x1.outp[ABOVE] = p;
+            x0.outp[ABOVE] = -1;
+          }
+          break;
+        case IRI:
+          if (q >= 0) {
+            add_right(A, q, ix, iy);
+            x0.outp[ABOVE] = q;
+            x1.outp[ABOVE] = -1;
+          }
+          break;
+        case IMX:
+          if (p >= 0 && q >= 0) {
+            add_right(A, p, ix, iy);
+            merge_left(A, p, q, out_poly);
+            x0.outp[ABOVE] = -1;
+            x1.outp[ABOVE] = -1;
+          }
+          break;
+        case IMM:
+          if (p >= 0 && q >= 0) {
+            add_right(A, p, ix, iy);
+            merge_left(A, p, q, out_poly);
+            add_local_min(A, out_poly, a0, ix, iy);
+            x1.outp[ABOVE] = x0.outp[ABOVE];
+          }
+          break;
+        case EMM:
+          if (p >= 0 && q >= 0) {
+            add_left(A, p, ix, iy);
+            merge_right(A, p, q, out_poly);
+            add_local_min(A, out_poly, a0, ix, iy);
+            x1.outp[ABOVE] = x0.outp[ABOVE];
+          }
+          break;
+        default:
+          break;
+      }
+    }
+    if (x0.bundle[ABOVE][CLIP]) x1.bside[CLIP] = !x1.bside[CLIP];
+    if (x1.bundle[ABOVE][CLIP]) x0.bside[CLIP] = !x0.bside[CLIP];
+    if (x0.bundle[ABOVE][SUBJ]) x1.bside[SUBJ] = !x1.bside[SUBJ];
+    if (x1.bundle[ABOVE][SUBJ]) x0.bside[SUBJ] = !x0.bside[SUBJ];
+    // swap the e0 and e1 bundles in the AET (GPC:622-657)
+    int pe = x0.prev, nx = x1.next;
+    if (nx >= 0) E[nx].prev = a0;
+    if (x0.bstate[ABOVE] == BUNDLE_HEAD) {
+      bool search = true;
+      int g5 = 0;
+      while (search) {
+        PRT_GUARD(g5, A.ne)
+        if (pe < 0) break;
+        pe = E[pe].prev;
+        if (pe >= 0) {
+          if (E[pe].bstate[ABOVE] != BUNDLE_TAIL) search = false;
+        } else {
+          search = false;
+        }
+      }
+    }
+    if (pe < 0) {
+      E[aet].prev = a1;
+      x1.next = aet;
+      aet = x0.next;
+    } else {
+      E[E[pe].next].prev = a1;
+      x1.next = E[pe].next;
+      E[pe].next = x0.next;
+    }
+    if (x0.next >= 0) E[x0.next].prev = pe;
+    if (x1.next >= 0) E[x1.next].prev = a1;
+    x0.next = nx;
+  }
+}
+
 __constant__ int8_t c_next_h[3][6] = {{BH, TH, TH, BH, NH, NH}, {NH, NH, NH, NH, TH, TH}, {NH, NH, NH, NH, BH, BH}};
 
 // Clips subj against clip.  Returns the head of the output polygon list
 // (-1 for an empty result); read it with count_result / write_result /
 // result_area.  A.status != kClipOk means the arena was too small.
-__device__ int clip_pair(Arena &A, int op, const PolyView &subj, const PolyView &clip) {
+static __device__ int clip_pair(Arena &A, int op, const PolyView &subj, const PolyView &clip) {
   const int sn = (int)(subj.r1 - subj.r0), cn = (int)(clip.r1 - clip.r0);
   if ((sn == 0 && cn == 0) || (sn == 0 && (op == OP_INT || op == OP_DIFF)) || (cn == 0 && op == OP_INT)) return -1;
 
@@ -534,10 +689,10 @@ __device__ int clip_pair(Arena &A, int op, const PolyView &subj, const PolyView 
   Edge *E = A.E;
   int parity[2] = {LEFT, LEFT};
   if (op == OP_DIFF) parity[CLIP] = RIGHT;
-  int aet = -1, it = -1, cf = -1, out_poly = -1;
+  int aet = -1, cf = -1, out_poly = -1;
   int lmin = 0, scanbeam = 0;
   double yb, yt = 0.0, dy = 0.0, px, xb;
-  int horiz[2], exists[2], in[2];
+  int horiz[2], exists[2];
 
   while (scanbeam < nsbt) {
     yb = A.Y[scanbeam++].y;
@@ -739,151 +894,7 @@ __device__ int clip_pair(Arena &A, int op, const PolyView &subj, const PolyView 
       }
     }
     if (scanbeam < nsbt) {
-      build_intersection_table(A, it, aet, dy);
-      if (A.status) return -1;
-      int g4 = 0;
-      for (int in_ = it; in_ >= 0 && !A.status; in_ = A.IT[in_].next) {
-        PRT_GUARD(g4, A.nit)
-        const int a0 = A.IT[in_].e0, a1 = A.IT[in_].e1;
-        Edge &x0 = E[a0];
-        Edge &x1 = E[a1];
-        if ((x0.bundle[ABOVE][CLIP] || x0.bundle[ABOVE][SUBJ]) && (x1.bundle[ABOVE][CLIP] || x1.bundle[ABOVE][SUBJ])) {
-          const int p = x0.outp[ABOVE], q = x1.outp[ABOVE];
-          const double ix = A.IT[in_].x;
-          const double iy = A.IT[in_].y + yb;
-          const int b0C = x0.bundle[ABOVE][CLIP], b0S = x0.bundle[ABOVE][SUBJ];
-          const int b1C = x1.bundle[ABOVE][CLIP], b1S = x1.bundle[ABOVE][SUBJ];
-          in[CLIP] = (b0C && !x0.bside[CLIP]) || (b1C && x1.bside[CLIP]) ||
-                     (!b0C && !b1C && x0.bside[CLIP] && x1.bside[CLIP]);
-          in[SUBJ] = (b0S && !x0.bside[SUBJ]) || (b1S && x1.bside[SUBJ]) ||
-                     (!b0S && !b1S && x0.bside[SUBJ] && x1.bside[SUBJ]);
-          int tr = 0, tl = 0, br = 0, bl = 0;
-          switch (op) {
-            case OP_DIFF:
-            case OP_INT:
-              tr = in[CLIP] && in[SUBJ];
-              tl = (in[CLIP] ^ b1C) && (in[SUBJ] ^ b1S);
-              br = (in[CLIP] ^ b0C) && (in[SUBJ] ^ b0S);
-              bl = (in[CLIP] ^ b1C ^ b0C) && (in[SUBJ] ^ b1S ^ b0S);
-              break;
-            case OP_XOR:
-              tr = in[CLIP] ^ in[SUBJ];
-              tl = (in[CLIP] ^ b1C) ^ (in[SUBJ] ^ b1S);
-              br = (in[CLIP] ^ b0C) ^ (in[SUBJ] ^ b0S);
-              bl = (in[CLIP] ^ b1C ^ b0C) ^ (in[SUBJ] ^ b1S ^ b0S);
-              break;
-            default:
-              tr = in[CLIP] || in[SUBJ];
-              tl = (in[CLIP] ^ b1C) || (in[SUBJ] ^ b1S);
-              br = (in[CLIP] ^ b0C) || (in[SUBJ] ^ b0S);
-              bl = (in[CLIP] ^ b1C ^ b0C) || (in[SUBJ] ^ b1S ^ b0S);
-              break;
-          }
-          const int vclass = tr + (tl << 1) + (br << 2) + (bl << 3);
-          switch (vclass) {
-            case EMN:
-            case IMN:
-              add_local_min(A, out_poly, a0, ix, iy);
-              x1.outp[ABOVE] = x0.outp[ABOVE];
-              break;
-            case ERI:
-              if (p >= 0) {
-                add_right(A, p, ix, iy);
-                x1.outp[ABOVE] = p;
-                x0.outp[ABOVE] = -1;
-              }
-              break;
-            case ELI:
-              if (q >= 0) {
-                add_left(A, q, ix, iy);
-                x0.outp[ABOVE] = q;
-                x1.outp[ABOVE] = -1;
-              }
-              break;
-            case EMX:
-              if (p >= 0 && q >= 0) {
-                add_left(A, p, ix, iy);
-                merge_right(A, p, q, out_poly);
-                x0.outp[ABOVE] = -1;
-                x1.outp[ABOVE] = -1;
-              }
-              break;
-            case ILI:
-              if (p >= 0) {
-                add_left(A, p, ix, iy);
-                x1.outp[ABOVE] = p;
-                x0.outp[ABOVE] = -1;
-              }
-              break;
-            case IRI:
-              if (q >= 0) {
-                add_right(A, q, ix, iy);
-                x0.outp[ABOVE] = q;
-                x1.outp[ABOVE] = -1;
-              }
-              break;
-            case IMX:
-              if (p >= 0 && q >= 0) {
-                add_right(A, p, ix, iy);
-                merge_left(A, p, q, out_poly);
-                x0.outp[ABOVE] = -1;
-                x1.outp[ABOVE] = -1;
-              }
-              break;
-            case IMM:
-              if (p >= 0 && q >= 0) {
-                add_right(A, p, ix, iy);
-                merge_left(A, p, q, out_poly);
-                add_local_min(A, out_poly, a0, ix, iy);
-                x1.outp[ABOVE] = x0.outp[ABOVE];
-              }
-              break;
-            case EMM:
-              if (p >= 0 && q >= 0) {
-                add_left(A, p, ix, iy);
-                merge_right(A, p, q, out_poly);
-                add_local_min(A, out_poly, a0, ix, iy);
-                x1.outp[ABOVE] = x0.outp[ABOVE];
-              }
-              break;
-            default:
-              break;
-          }
-        }
-        if (x0.bundle[ABOVE][CLIP]) x1.bside[CLIP] = !x1.bside[CLIP];
-        if (x1.bundle[ABOVE][CLIP]) x0.bside[CLIP] = !x0.bside[CLIP];
-        if (x0.bundle[ABOVE][SUBJ]) x1.bside[SUBJ] = !x1.bside[SUBJ];
-        if (x1.bundle[ABOVE][SUBJ]) x0.bside[SUBJ] = !x0.bside[SUBJ];
-        // swap the e0 and e1 bundles in the AET (GPC:622-657)
-        int pe = x0.prev, nx = x1.next;
-        if (nx >= 0) E[nx].prev = a0;
-        if (x0.bstate[ABOVE] == BUNDLE_HEAD) {
-          bool search = true;
-          int g5 = 0;
-          while (search) {
-            PRT_GUARD(g5, A.ne)
-            if (pe < 0) break;
-            pe = E[pe].prev;
-            if (pe >= 0) {
-              if (E[pe].bstate[ABOVE] != BUNDLE_TAIL) search = false;
-            } else {
-              search = false;
-            }
-          }
-        }
-        if (pe < 0) {
-          E[aet].prev = a1;
-          x1.next = aet;
-          aet = x0.next;
-        } else {
-          E[E[pe].next].prev = a1;
-          x1.next = E[pe].next;
-          E[pe].next = x0.next;
-        }
-        if (x0.next >= 0) E[x0.next].prev = pe;
-        if (x1.next >= 0) E[x1.next].prev = a1;
-        x0.next = nx;
-      }
+      intersect_beam(A, op, aet, out_poly, yb, dy);
       if (A.status) return -1;
       // prepare for the next scanbeam (GPC:661-693)
       int nx;

@@ -203,6 +203,24 @@ TreeLevels level_layout(int64_t n, int fanout);
 
 }  // namespace prt
 
+struct prt_tree;
+
+namespace prt {
+
+// Capture-safe pieces of the pipeline (no host synchronisation inside):
+// tree_alloc allocates a tree's storage for n boxes; bu_enqueue enqueues its
+// bottom-up build; join_enqueue enqueues a breadth-first join with caller-owned
+// frontier buffers and counters (counters: PRT_MAX_LEVELS + 2 uint64, zeroed by
+// the caller; [l] = frontier items entering node level l-1, [PRT_MAX_LEVELS] =
+// pairs found, all counted even past the capacities).
+int tree_alloc(const void *d_boxes, int coord, int64_t n, int fanout, int kind, int key_mode, cudaStream_t s,
+               prt_tree **out);
+int bu_enqueue(prt_tree *t, const void *d_boxes, const int32_t *d_ids, unsigned *d_err, cudaStream_t s);
+int join_enqueue(const prt_tree *t, const void *d_queries, int64_t nq, uint2 *d_pairs, int64_t cap, uint2 *fr0,
+                 uint2 *fr1, int64_t fcap, unsigned long long *d_counters, cudaStream_t s);
+
+}  // namespace prt
+
 struct prt_tree {
   int kind;
   int coord;

@@ -429,3 +429,44 @@ int prt_join_noalloc(const prt_tree *t, const void *d_queries, int coord_type, i
 }
 
 }  // extern "C"
+
+namespace prt {
+
+// Breadth-first join into caller-owned buffers, nothing synchronised: the
+// capture-safe form used by the graph pipeline (prt_pipeline_*).
+int join_enqueue(const prt_tree *t, const void *d_queries, int64_t nq, uint2 *d_pairs, int64_t cap, uint2 *fr0,
+                 uint2 *fr1, int64_t fcap, unsigned long long *cnt, cudaStream_t s) {
+  PRT_CHECK(t != nullptr && nq >= 0, PRT_ERR_INVALID, "join_enqueue arguments");
+  if (nq == 0) return PRT_OK;
+  const TreeLevels &L = t->lv;
+  const size_t bs = 4 * coord_size(t->coord);
+  uint2 *fr[2] = {fr0, fr1};
+  int cur = -1;
+  int rc = PRT_OK;
+  for (int l = L.levels - 1; l >= 0 && !rc; l--) {
+    JoinLevel J;
+    J.mbr = reinterpret_cast<const char *>(t->d_mbr) + L.offset[l] * bs;
+    J.n_entries = L.count[l];
+    J.in = cur < 0 ? nullptr : fr[cur];
+    J.in_count = cur < 0 ? nullptr : &cnt[l + 1];
+    J.in_cap = fcap;
+    J.leaf = l == 0;
+    int nxt = cur < 0 ? 0 : 1 - cur;
+    J.out = J.leaf ? d_pairs : fr[nxt];
+    J.out_count = J.leaf ? &cnt[PRT_MAX_LEVELS] : &cnt[l];
+    J.out_cap = J.leaf ? cap : fcap;
+    J.nq = nq;
+    J.counts = nullptr;
+    J.td_slots = 0;
+    rc = dispatch_coord(t->coord, [&](auto tag) {
+      using T = decltype(tag);
+      return launch_expand<T>(J, d_queries, t->fanout, s);
+    });
+    cur = nxt;
+  }
+  if (rc) return rc;
+  PRT_CUDA(cudaGetLastError());
+  return PRT_OK;
+}
+
+}  // namespace prt

@@ -18,9 +18,12 @@
 #include <algorithm>
 #include <vector>
 
+#include <mutex>
+
 #include "prt_gpc.cuh"
 #include "prt_internal.cuh"
 #include "prt_overlay.cuh"
+#include "prt_wgpc.cuh"
 
 namespace prt {
 
@@ -65,18 +68,9 @@ __device__ inline bool resolve(const PairSrc &S, int64_t i, gpc::PolyView &a, gp
   return true;
 }
 
-__device__ void process_pair(const PairSrc &S, const ClipOut &O, int64_t i, unsigned char *slice, int scale) {
-  gpc::PolyView a, b;
-  int64_t nv = 0;
-  if (!resolve(S, i, a, b, nv)) {
-    O.status[i] = kPairInvalid;
-    if (O.pair_ncont) O.pair_ncont[i] = 0;
-    if (O.area) O.area[i] = 0.0;
-    return;
-  }
-  gpc::Arena A;
-  gpc::arena_init(A, slice, gpc::caps_for(nv, scale));
-  int head = gpc::clip_pair(A, S.op, a, b);
+// Records the clip result of pair i (arena A, output list head): per-pair
+// area, or contours and vertices reserved from the result pools.
+__device__ void finish_pair(const ClipOut &O, int64_t i, gpc::Arena &A, int head) {
   int nc = 0;
   int64_t nvt = 0;
   if (!A.status) gpc::count_result(A, head, &nc, &nvt);
@@ -108,6 +102,55 @@ __device__ void process_pair(const PairSrc &S, const ClipOut &O, int64_t i, unsi
   O.status[i] = kPairOk;
 }
 
+__device__ inline void invalid_pair(const ClipOut &O, int64_t i) {
+  O.status[i] = kPairInvalid;
+  if (O.pair_ncont) O.pair_ncont[i] = 0;
+  if (O.area) O.area[i] = 0.0;
+}
+
+// One pair on the calling thread.
+__device__ void process_pair(const PairSrc &S, const ClipOut &O, int64_t i, unsigned char *slice, int scale) {
+  gpc::PolyView a, b;
+  int64_t nv = 0;
+  if (!resolve(S, i, a, b, nv)) {
+    invalid_pair(O, i);
+    return;
+  }
+  gpc::Arena A;
+  gpc::arena_init(A, slice, gpc::caps_for(nv, scale));
+  int head = gpc::clip_pair(A, S.op, a, b);
+  finish_pair(O, i, A, head);
+}
+
+// One pair on the calling warp (all lanes): the warp clipper, or the thread
+// clipper on lane 0 when the pair outgrows the warp's active-edge slots.
+__device__ void process_pair_warp(const PairSrc &S, const ClipOut &O, int64_t i, unsigned char *slice, int scale,
+                                  gpc::WAet &W, unsigned long long *fallbacks) {
+  const int lane = threadIdx.x & 31;
+  gpc::PolyView a, b;
+  int64_t nv = 0;
+  if (!resolve(S, i, a, b, nv)) {
+    if (lane == 0) invalid_pair(O, i);
+    __syncwarp();
+    return;
+  }
+  gpc::Arena A;
+  const gpc::Caps caps = gpc::caps_for(nv, scale);
+  gpc::arena_init(A, slice, caps);
+  int mode = gpc::kWarpOk;
+  int head = gpc::wclip_pair(A, S.op, a, b, W, &mode);
+  __syncwarp();
+  if (lane == 0) {
+    if (mode == gpc::kWarpFallback) {
+      if (fallbacks) atomicAdd(fallbacks, 1ull);
+      gpc::arena_init(A, slice, caps);
+      head = gpc::clip_pair(A, S.op, a, b);
+    }
+    finish_pair(O, i, A, head);
+  }
+  __syncwarp();
+}
+
 namespace {
 
 __global__ void nv_kernel(PairSrc S, int64_t n, const int64_t *__restrict__ idx, int scale, int64_t *__restrict__ nv,
@@ -133,21 +176,52 @@ __global__ void __launch_bounds__(128) clip_plain_kernel(PairSrc S, ClipOut O, c
   process_pair(S, O, i, arena + (arena_off[k] - off_base), scale);
 }
 
-__global__ void __launch_bounds__(128) clip_batched_kernel(PairSrc S, ClipOut O, const uint32_t *__restrict__ order,
-                                                           int64_t begin, int64_t end,
-                                                           unsigned long long *ticket, unsigned char *arena,
-                                                           size_t slice_bytes, int64_t workers, int scale) {
+// One persistent launch over all bins (longest pairs first): each warp drains
+// its own bin from the bin's atomic ticket (one pair per ticket in warp mode,
+// 32 in thread mode), then steals from the smaller bins after it.  One warp
+// per block spreads the big-pair warps over every SM; the block's dynamic
+// shared memory holds the warp clipper's active-edge slots.
+__global__ void __launch_bounds__(32) clip_lpt_kernel(PairSrc S, ClipOut O, const uint32_t *__restrict__ order,
+                                                      BinPlan plan, unsigned long long *tickets,
+                                                      unsigned char *arena, int scale,
+                                                      const int64_t *__restrict__ dyn_ranges) {
+  extern __shared__ __align__(16) unsigned char wsm[];
   const int lane = threadIdx.x & 31;
-  const int64_t worker = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (worker >= workers) return;  // workers is a multiple of 32: whole warps leave
-  unsigned char *slice = arena + worker * slice_bytes;
-  for (;;) {
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(ticket, 32ull);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    int64_t k = begin + (int64_t)base + lane;
-    if (begin + (int64_t)base >= end) break;
-    if (k < end) process_pair(S, O, (int64_t)order[k], slice, scale);
+  const int64_t w = blockIdx.x;
+  if (dyn_ranges) {  // bin ranges computed on the device (graph mode)
+    for (int b = 0; b < plan.nbins; b++) {
+      plan.begin[b] = dyn_ranges[2 * b];
+      plan.end[b] = dyn_ranges[2 * b + 1];
+    }
+  }
+  gpc::WAet W = gpc::waet_carve(wsm, plan.wcap);
+  int g = 0;
+  while (g + 1 < plan.nbins && w >= plan.warp0[g + 1]) g++;
+  unsigned char *region = arena + plan.arena_off[g] + (w - plan.warp0[g]) * plan.region[g];
+  unsigned char *slice = region + (int64_t)lane * ((plan.region[g] / 32) & ~(int64_t)15);
+  unsigned long long *fallbacks = tickets + PRT_MAX_BINS;
+  for (int b = g; b < plan.nbins; b++) {
+    if (plan.warp_mode[b]) {
+      for (;;) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(&tickets[b], 1ull);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        const int64_t k = plan.begin[b] + (int64_t)t;
+        if (k >= plan.end[b]) break;
+        process_pair_warp(S, O, (int64_t)order[k], region, scale, W, fallbacks);
+      }
+    } else {
+      for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&tickets[b], 32ull);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        const int64_t k0 = plan.begin[b] + (int64_t)base;
+        if (k0 >= plan.end[b]) break;
+        const int64_t k = k0 + lane;
+        if (k < plan.end[b]) process_pair(S, O, (int64_t)order[k], slice, scale);
+        __syncwarp();
+      }
+    }
   }
 }
 
@@ -246,9 +320,87 @@ size_t arena_budget() {
 
 }  // namespace
 
-// Bins for the batched schedule: upper bounds on the pair vertex count.
-static const int64_t kBinThresholds[] = {1ll << 40, 4096, 1024, 256, 64};
-static const int kNumBins = 5;
+// ---- batched schedule ----------------------------------------------------------
+// Default: pairs above 256 vertices are clipped one per warp, smaller ones one
+// per thread; the warps per SM of all bins add up to what the SM holds at the
+// default slot count.
+static prt_schedule default_schedule() {
+  prt_schedule d;
+  memset(&d, 0, sizeof d);
+  d.nbins = 5;
+  d.aet_slots = 256;
+  const int64_t thr[5] = {1ll << 40, 4096, 1024, 256, 64};
+  const int32_t wm[5] = {1, 1, 1, 0, 0};
+  const int32_t wps[5] = {4, 3, 3, 2, 2};
+  for (int b = 0; b < 5; b++) {
+    d.bin_thresholds[b] = thr[b];
+    d.bin_warp_mode[b] = wm[b];
+    d.bin_warps_per_sm[b] = wps[b];
+  }
+  return d;
+}
+
+static std::mutex g_sched_mu;
+static prt_schedule g_sched = default_schedule();
+
+prt_schedule current_schedule() {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  return g_sched;
+}
+
+int schedule_valid(const prt_schedule &s) {
+  PRT_CHECK(s.nbins >= 1 && s.nbins <= PRT_MAX_BINS, PRT_ERR_INVALID, "schedule: nbins %d", s.nbins);
+  PRT_CHECK(s.aet_slots >= 32 && s.aet_slots <= 2048 && s.aet_slots % 32 == 0, PRT_ERR_INVALID,
+            "schedule: aet_slots %d (a multiple of 32 in [32, 2048])", s.aet_slots);
+  for (int b = 0; b < s.nbins; b++) {
+    PRT_CHECK(s.bin_thresholds[b] > 0, PRT_ERR_INVALID, "schedule: threshold %d", b);
+    PRT_CHECK(b == 0 || s.bin_thresholds[b] < s.bin_thresholds[b - 1], PRT_ERR_INVALID,
+              "schedule: thresholds must descend");
+    PRT_CHECK(s.bin_warps_per_sm[b] >= 1 && s.bin_warps_per_sm[b] <= 64, PRT_ERR_INVALID,
+              "schedule: warps per SM of bin %d", b);
+    PRT_CHECK(s.bin_warp_mode[b] == 0 || s.bin_warp_mode[b] == 1, PRT_ERR_INVALID, "schedule: warp mode of bin %d",
+              b);
+  }
+  PRT_CHECK(s.bin_thresholds[0] >= (1ll << 31), PRT_ERR_INVALID, "schedule: bin 0 must hold every pair size");
+  return PRT_OK;
+}
+
+size_t plan_bins(const prt_schedule &sc, const int64_t *counts, const int64_t *maxnv, size_t budget, BinPlan &plan,
+                 size_t *smem) {
+  memset(&plan, 0, sizeof plan);
+  plan.nbins = sc.nbins;
+  plan.wcap = sc.aet_slots;
+  int64_t need[PRT_MAX_BINS];
+  bool any_warp = false;
+  for (int b = 0; b < sc.nbins; b++) {
+    const int64_t sl = (int64_t)gpc::align16(gpc::arena_bytes(gpc::caps_for(maxnv[b] > 0 ? maxnv[b] : 4, 1)));
+    plan.warp_mode[b] = sc.bin_warp_mode[b];
+    need[b] = counts[b] > 0 ? (sc.bin_warp_mode[b] ? sl : 32 * sl) : 0;
+    any_warp |= sc.bin_warp_mode[b] && counts[b] > 0;
+  }
+  size_t bytes = 0;
+  int64_t warps = 0;
+  for (int g = 0; g < sc.nbins; g++) {
+    int64_t region = 512;
+    for (int b = g; b < sc.nbins; b++) region = std::max(region, need[b]);
+    region = (region + 511) & ~(int64_t)511;
+    int64_t wg = 0;
+    if (counts[g] > 0) {
+      const int64_t per = sc.bin_warp_mode[g] ? 1 : 32;
+      wg = std::min<int64_t>((counts[g] + per - 1) / per, (int64_t)kSMs * sc.bin_warps_per_sm[g]);
+      const int64_t mem_cap = (int64_t)((budget - std::min(budget, bytes)) / (size_t)region);
+      wg = std::max<int64_t>(1, std::min(wg, mem_cap));
+    }
+    plan.warp0[g] = warps;
+    plan.arena_off[g] = (int64_t)bytes;
+    plan.region[g] = region;
+    bytes += (size_t)wg * (size_t)region;
+    warps += wg;
+  }
+  plan.warp0[sc.nbins] = warps;
+  *smem = any_warp ? gpc::waet_bytes(sc.aet_slots) : 0;
+  return bytes;
+}
 
 struct OverlayState {
   PairSrc S;
@@ -359,26 +511,36 @@ static int run_plain(OverlayState &st, const int64_t *d_idx, int64_t count, int 
   return rc;
 }
 
+// Lets the persistent clip kernel take `smem` bytes of dynamic shared memory
+// (the warp clipper's slots); called before any launch or capture.
+int prepare_lpt_launch(size_t smem) {
+  if (smem > 48 * 1024)
+    PRT_CUDA(cudaFuncSetAttribute(clip_lpt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  return PRT_OK;
+}
+
 static int run_batched(OverlayState &st, cudaStream_t s) {
   const int64_t n = st.n;
+  const prt_schedule sc = current_schedule();
+  const int nb = sc.nbins;
   int64_t *nv = nullptr;
   unsigned char *scr = nullptr;
   int rc = dalloc(&nv, n, s);
-  if (!rc) rc = dmalloc(reinterpret_cast<void **>(&scr), 256 + 16 * n + 4 * n, s);
+  if (!rc) rc = dmalloc(reinterpret_cast<void **>(&scr), 512 + 16 * n + 4 * n, s);
   if (rc) {
     dfree(nv, s);
     return rc;
   }
   unsigned *err = reinterpret_cast<unsigned *>(scr);
   int *sel = reinterpret_cast<int *>(scr + 8);
-  int64_t *thr = reinterpret_cast<int64_t *>(scr + 16);   // kNumBins
-  int64_t *bnd = thr + 8;                                 // kNumBins
-  int64_t *mx = bnd + 8;                                  // kNumBins
-  unsigned long long *tickets = reinterpret_cast<unsigned long long *>(mx + 8);  // kNumBins
-  uint32_t *k0 = reinterpret_cast<uint32_t *>(scr + 256);
+  int64_t *thr = reinterpret_cast<int64_t *>(scr + 16);                            // PRT_MAX_BINS
+  int64_t *bnd = thr + PRT_MAX_BINS;                                               // PRT_MAX_BINS
+  int64_t *mx = bnd + PRT_MAX_BINS;                                                // PRT_MAX_BINS
+  unsigned long long *tickets = reinterpret_cast<unsigned long long *>(mx + PRT_MAX_BINS);  // bins + fallbacks
+  uint32_t *k0 = reinterpret_cast<uint32_t *>(scr + 512);
   uint32_t *k1 = k0 + n, *v0 = k1 + n, *v1 = v0 + n, *order = v1 + n;
-  cudaMemsetAsync(scr, 0, 256, s);
-  cudaMemcpyAsync(thr, kBinThresholds, sizeof(int64_t) * kNumBins, cudaMemcpyHostToDevice, s);
+  cudaMemsetAsync(scr, 0, 512, s);
+  cudaMemcpyAsync(thr, sc.bin_thresholds, sizeof(int64_t) * nb, cudaMemcpyHostToDevice, s);
   const int g = grid_for(n, 256, 16);
   {
     PRT_PROF("nv", s);
@@ -389,7 +551,7 @@ static int run_batched(OverlayState &st, cudaStream_t s) {
     size_key_kernel<<<g, 256, 0, s>>>(nv, n, k0, v0);
   }
   rc = radix_sort_pairs<uint32_t>(k0, v0, k1, v1, n, 32, sel, err, s);
-  int64_t hb[8] = {0}, hm[8] = {0};
+  int64_t hb[PRT_MAX_BINS + 1] = {0}, hm[PRT_MAX_BINS] = {0};
   if (!rc) {
     {
       PRT_PROF("select_u32", s);
@@ -397,40 +559,31 @@ static int run_batched(OverlayState &st, cudaStream_t s) {
     }
     {
       PRT_PROF("bin_bounds", s);
-      bin_bounds_kernel<<<1, 32, 0, s>>>(k0, k1, sel, n, thr, kNumBins, bnd, mx);
+      bin_bounds_kernel<<<1, 32, 0, s>>>(k0, k1, sel, n, thr, nb, bnd, mx);
     }
-    cudaMemcpyAsync(hb, bnd, sizeof(int64_t) * kNumBins, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(hm, mx, sizeof(int64_t) * kNumBins, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hb, bnd, sizeof(int64_t) * nb, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hm, mx, sizeof(int64_t) * nb, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) rc = cuda_status(e, "overlay batched");
   }
-  // bin b covers sorted positions [bnd[b], bnd[b+1]) (bnd[kNumBins] = n)
-  hb[kNumBins] = n;
-  const size_t budget = arena_budget();
-  const int64_t resident = (int64_t)kSMs * 1024;
+  // bin b covers sorted positions [bnd[b], bnd[b+1]) (bnd[nbins] = n)
+  hb[nb] = n;
+  BinPlan plan;
+  int64_t counts[PRT_MAX_BINS];
+  for (int b = 0; b < nb; b++) counts[b] = hb[b + 1] - hb[b];
+  size_t smem = 0;
+  const size_t bytes = plan_bins(sc, counts, hm, arena_budget(), plan, &smem);
+  for (int b = 0; b < nb; b++) {
+    plan.begin[b] = hb[b];
+    plan.end[b] = hb[b + 1];
+  }
+  const int64_t warps = plan.warp0[nb];
   unsigned char *arena = nullptr;
-  size_t arena_cap = 0;
-  for (int bi = 0; bi < kNumBins && !rc; bi++) {
-    int64_t b0 = hb[bi], b1 = hb[bi + 1];
-    if (b1 <= b0) continue;
-    const int64_t maxnv = hm[bi];
-    const size_t slice = gpc::arena_bytes(gpc::caps_for(maxnv, 1));
-    int64_t workers = std::min<int64_t>(b1 - b0, resident);
-    workers = std::min<int64_t>(workers, (int64_t)(budget / slice));
-    workers = std::max<int64_t>(32, (workers + 31) / 32 * 32);
-    size_t need = slice * (size_t)workers;
-    if (need > arena_cap) {
-      dfree(arena, s);
-      arena = nullptr;
-      rc = dmalloc(reinterpret_cast<void **>(&arena), need, s);
-      if (rc) break;
-      arena_cap = need;
-    }
-    {
-      PRT_PROF("clip_batched", s);
-      clip_batched_kernel<<<(unsigned)((workers + 127) / 128), 128, 0, s>>>(st.S, st.O, order, b0, b1, &tickets[bi],
-                                                                          arena, slice, workers, 1);
-    }
+  if (!rc) rc = prepare_lpt_launch(smem);
+  if (!rc && warps > 0) rc = dmalloc(reinterpret_cast<void **>(&arena), bytes, s);
+  if (!rc && warps > 0) {
+    PRT_PROF("clip_batched", s);
+    clip_lpt_kernel<<<(unsigned)warps, 32, smem, s>>>(st.S, st.O, order, plan, tickets, arena, 1, nullptr);
   }
   if (!rc) {
     cudaError_t e = cudaGetLastError();
@@ -511,6 +664,130 @@ static int retry_failed(OverlayState &st, cudaStream_t s) {
   return PRT_ERR_CAPACITY;
 }
 
+// ---- capture-safe overlay (graph pipeline) ----------------------------------
+
+// Size keys of the first *d_count pairs (larger first); the padding slots up to
+// cap sort last.
+__global__ void graph_size_key_kernel(PairSrc S, const unsigned long long *__restrict__ d_count, int64_t cap,
+                                      uint32_t *__restrict__ key, uint32_t *__restrict__ val) {
+  const int64_t count = (int64_t)min((unsigned long long)cap, *d_count);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cap; i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t k = 0xFFFFFFFFu;
+    if (i < count) {
+      gpc::PolyView a, b;
+      int64_t v = 0;
+      if (!resolve(S, i, a, b, v)) v = 0;
+      if (v > 0xFFFFFFFEll) v = 0xFFFFFFFEll;
+      k = 0xFFFFFFFEu - (uint32_t)v;
+    }
+    key[i] = k;
+    val[i] = (uint32_t)i;
+  }
+}
+
+// ranges[2b], ranges[2b+1]: sorted positions of bin b among the first count
+__global__ void graph_bins_kernel(const uint32_t *__restrict__ k0, const uint32_t *__restrict__ k1,
+                                  const int *__restrict__ sel, const unsigned long long *__restrict__ d_count,
+                                  int64_t cap, const int64_t *__restrict__ thr, int nbins, int64_t *__restrict__ ranges) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const uint32_t *k = *sel ? k1 : k0;
+  const int64_t count = (int64_t)min((unsigned long long)cap, *d_count);
+  int64_t lo_prev = 0;
+  for (int b = 0; b < nbins; b++) {
+    int64_t lo = 0, hi = count;
+    while (lo < hi) {
+      int64_t mid = (lo + hi) / 2;
+      int64_t v = (int64_t)(0xFFFFFFFEu - k[mid]);
+      if (v > thr[b]) lo = mid + 1;
+      else hi = mid;
+    }
+    if (b > 0) ranges[2 * (b - 1) + 1] = lo;
+    ranges[2 * b] = lo;
+    lo_prev = lo;
+  }
+  ranges[2 * (nbins - 1) + 1] = count;
+  (void)lo_prev;
+}
+
+__global__ void graph_totals_kernel(const int64_t *__restrict__ pair_cstart, const int32_t *__restrict__ pair_ncont,
+                                    const int32_t *__restrict__ cont_nverts, const int32_t *__restrict__ status,
+                                    const unsigned long long *__restrict__ d_count, int64_t cap,
+                                    unsigned long long *__restrict__ tot) {
+  const int64_t n = (int64_t)min((unsigned long long)cap, *d_count);
+  unsigned long long c = 0, v = 0, ne = 0, bad = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (status[i] != kPairOk) {
+      bad++;
+      continue;
+    }
+    int k = pair_ncont[i];
+    c += k;
+    ne += k > 0;
+    for (int j = 0; j < k; j++) v += cont_nverts[pair_cstart[i] + j];
+  }
+  for (int o = 16; o; o >>= 1) {
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+    ne += __shfl_xor_sync(0xffffffffu, ne, o);
+    bad += __shfl_xor_sync(0xffffffffu, bad, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&tot[0], c);
+    atomicAdd(&tot[1], v);
+    atomicAdd(&tot[2], ne);
+    atomicAdd(&tot[3], bad);
+  }
+}
+
+int overlay_graph_enqueue(const PairSrc &S, const unsigned long long *d_npairs, GraphOverlay &G, cudaStream_t s) {
+  const int64_t cap = G.cap_pairs;
+  PRT_CUDA(cudaMemsetAsync(G.status, 0, 4 * cap, s));
+  PRT_CUDA(cudaMemsetAsync(G.pair_ncont, 0, 4 * cap, s));
+  PRT_CUDA(cudaMemsetAsync(G.tickets, 0, 8 * (PRT_MAX_BINS + 1), s));
+  PRT_CUDA(cudaMemsetAsync(G.pool, 0, 16, s));
+  PRT_CUDA(cudaMemsetAsync(G.totals, 0, 32, s));
+  PRT_CUDA(cudaMemsetAsync(G.err, 0, 4, s));
+  const int g = grid_for(cap, 256, 16);
+  {
+    PRT_PROF("size_key", s);
+    graph_size_key_kernel<<<g, 256, 0, s>>>(S, d_npairs, cap, G.k0, G.v0);
+  }
+  int rc = radix_sort_pairs<uint32_t>(G.k0, G.v0, G.k1, G.v1, cap, 32, G.sel, G.err, s);
+  if (rc) return rc;
+  {
+    PRT_PROF("select_u32", s);
+    select_u32_kernel<<<g, 256, 0, s>>>(G.v0, G.v1, G.sel, cap, G.order);
+  }
+  {
+    PRT_PROF("bin_bounds", s);
+    graph_bins_kernel<<<1, 32, 0, s>>>(G.k0, G.k1, G.sel, d_npairs, cap, G.thresholds, G.plan.nbins, G.ranges);
+  }
+  ClipOut O;
+  memset(&O, 0, sizeof O);
+  O.status = G.status;
+  O.pair_cstart = G.pair_cstart;
+  O.pair_ncont = G.pair_ncont;
+  O.cont_vstart = G.cont_vstart;
+  O.cont_nverts = G.cont_nverts;
+  O.cont_hole = G.cont_hole;
+  O.xy = G.xy;
+  O.pool = G.pool;
+  O.cap_c = G.cap_c;
+  O.cap_v = G.cap_v;
+  const int64_t warps = G.plan.warp0[G.plan.nbins];
+  if (warps > 0) {
+    PRT_PROF("clip_batched", s);
+    clip_lpt_kernel<<<(unsigned)warps, 32, G.smem, s>>>(S, O, G.order, G.plan, G.tickets, G.arena, 1, G.ranges);
+  }
+  {
+    PRT_PROF("result_totals", s);
+    graph_totals_kernel<<<grid_for(cap, 256, 8), 256, 0, s>>>(G.pair_cstart, G.pair_ncont, G.cont_nverts, G.status,
+                                                             d_npairs, cap, G.totals);
+  }
+  PRT_CUDA(cudaGetLastError());
+  return PRT_OK;
+}
+
 }  // namespace prt
 
 struct prt_results {
@@ -573,8 +850,10 @@ int overlay_impl(const PairSrc &S, int64_t n, int sched, double *d_area, cudaStr
     dfree(tmp, s);
   }
   if (!rc && !d_area) {
-    st.O.cap_c = total_nv / 4 + 1024;
-    st.O.cap_v = total_nv + 4096;
+    // first guess at the result size (grown on demand): a quarter of the input
+    // vertices, one contour per 64 of them
+    st.O.cap_c = total_nv / 64 + 1024;
+    st.O.cap_v = total_nv / 4 + 4096;
     rc = dalloc(&st.O.cont_vstart, st.O.cap_c, s);
     if (!rc) rc = dalloc(&st.O.cont_nverts, st.O.cap_c, s);
     if (!rc) rc = dalloc(&st.O.cont_hole, st.O.cap_c, s);
@@ -649,6 +928,22 @@ __global__ void ring_vert_from_ref_kernel(const int32_t *num, const int64_t *pre
 using namespace prt;
 
 extern "C" {
+
+int prt_schedule_set(const prt_schedule *sched) {
+  prt_schedule s = sched ? *sched : prt::default_schedule();
+  int rc = prt::schedule_valid(s);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(prt::g_sched_mu);
+  prt::g_sched = s;
+  return PRT_OK;
+}
+
+int prt_schedule_get(prt_schedule *sched) {
+  PRT_CHECK(sched != nullptr, PRT_ERR_INVALID, "NULL argument");
+  *sched = prt::current_schedule();
+  return PRT_OK;
+}
+
 
 int prt_overlay_run(const prt_pair *d_pairs, int64_t n_pairs, int32_t offset, const int32_t *d_leaf_to_poly,
                     const prt_layer *base, const prt_layer *overlay, int op, int sched, void *stream,

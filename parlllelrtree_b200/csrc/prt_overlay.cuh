@@ -43,3 +43,66 @@ inline LayerDev layer_dev(const prt_layer *l) {
 int overlay_impl(const PairSrc &S, int64_t n, int sched, double *d_area, cudaStream_t s, prt_results **out);
 
 }  // namespace prt
+
+namespace prt {
+
+// Bins of the batched schedule, size-descending: bin b holds sorted positions
+// [begin[b], end[b]); warps [warp0[g], warp0[g+1]) start on bin g, each with
+// region[g] bytes of arena (enough for one pair of bin g or any later bin in
+// warp mode, or 32 pairs in thread mode), then steal from the later bins.
+struct BinPlan {
+  int64_t begin[PRT_MAX_BINS], end[PRT_MAX_BINS];
+  int64_t warp0[PRT_MAX_BINS + 1];
+  int64_t region[PRT_MAX_BINS];
+  int64_t arena_off[PRT_MAX_BINS];
+  int32_t warp_mode[PRT_MAX_BINS];
+  int nbins;
+  int wcap;  // AET slots per warp (warp mode)
+};
+
+// The schedule of the calling process (prt_schedule_set).
+prt_schedule current_schedule();
+// PRT_OK, or PRT_ERR_INVALID with the reason as the last error.
+int schedule_valid(const prt_schedule &s);
+// Fills plan for bins with at most counts[b] pairs of at most maxnv[b]
+// vertices, arena limited to `budget` bytes; returns the arena bytes and the
+// dynamic shared memory per block in *smem.
+size_t plan_bins(const prt_schedule &sc, const int64_t *counts, const int64_t *maxnv, size_t budget, BinPlan &plan,
+                 size_t *smem);
+
+// Allows the persistent clip kernel `smem` bytes of dynamic shared memory.
+int prepare_lpt_launch(size_t smem);
+
+// Buffers of the capture-safe (CUDA graph) overlay: everything preallocated
+// for at most cap_pairs pairs, sizes read from device memory at run time.
+struct GraphOverlay {
+  int64_t cap_pairs = 0;
+  uint32_t *k0 = nullptr, *k1 = nullptr, *v0 = nullptr, *v1 = nullptr, *order = nullptr;
+  int *sel = nullptr;
+  unsigned *err = nullptr;
+  int64_t *ranges = nullptr;              // [2 * bins] begin/end per bin (device)
+  int64_t *thresholds = nullptr;          // [bins] vertex-count upper bounds (device)
+  unsigned long long *tickets = nullptr;  // [bins]
+  unsigned long long *totals = nullptr;   // [4] contours, vertices, non-empty, failed pairs
+  unsigned char *arena = nullptr;
+  size_t arena_bytes = 0;
+  BinPlan plan;
+  size_t smem = 0;
+  // results
+  int32_t *status = nullptr;
+  int64_t *pair_cstart = nullptr;
+  int32_t *pair_ncont = nullptr;
+  int64_t *cont_vstart = nullptr;
+  int32_t *cont_nverts = nullptr;
+  int32_t *cont_hole = nullptr;
+  double *xy = nullptr;
+  unsigned long long *pool = nullptr;     // [2] contours, vertices reserved
+  int64_t cap_c = 0, cap_v = 0;
+};
+
+// Enqueues the batched overlay of the first *d_npairs pairs (at most
+// G.cap_pairs) with no host synchronisation: zero the counters, size keys,
+// size sort, bin ranges, one longest-first persistent launch, result totals.
+int overlay_graph_enqueue(const PairSrc &S, const unsigned long long *d_npairs, GraphOverlay &G, cudaStream_t s);
+
+}  // namespace prt

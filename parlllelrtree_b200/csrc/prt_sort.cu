@@ -301,7 +301,15 @@ int radix_sort_pairs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1,
       plan_kernel<<<1, kRadix, 0, s>>>(ghist, goff, passes, n, plan, d_sel);
     }
     size_t smem = sizeof(PassSmem<KeyT>);
-    e = cudaFuncSetAttribute(onesweep_pass<KeyT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the shared-memory opt-in is set once per device (not a stream
+    // operation, but kept out of graph captures after the first call)
+    static bool attr_done[256] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 256 || !attr_done[dev]) {
+      e = cudaFuncSetAttribute(onesweep_pass<KeyT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess && dev >= 0 && dev < 256) attr_done[dev] = true;
+    }
     for (int p = 0; p < passes && e == cudaSuccess; p++) {
       {
         PRT_PROF("onesweep_pass", s);

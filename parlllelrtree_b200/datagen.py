@@ -255,12 +255,13 @@ def layer_bboxes(layer: dict) -> np.ndarray:
 
 def star_layer_device(n: int, seed: int, nv_lo: int = 4, nv_hi: int = 4096, r_lo: float = 1e-3,
                       r_hi: float = 1e-2, zipf: float | None = 1.2, hole_frac: float = 0.05,
-                      centres: str = "mixture", device: str = "cuda") -> dict:
+                      centres: str = "mixture", device: str = "cuda", chunk: int = 1 << 16) -> dict:
     """``star_layer`` for large layers: the per-polygon draws (vertex counts,
-    radii, centres, holes) come from numpy exactly as in ``star_layer``, the
-    per-vertex draws and trigonometry run in torch on ``device``.  Returns the
-    same dict with torch tensors on the device.  Same distribution as
-    ``star_layer``, not the same numbers."""
+    radii, centres, holes, lobes) come from numpy, the per-vertex draws and
+    trigonometry run in torch on ``device``, ``chunk`` polygons at a time so
+    the temporaries stay a few GB for any layer size.  Returns the same dict
+    with torch tensors on the device.  Same distribution as ``star_layer``,
+    not the same numbers."""
     import torch
 
     rng = np.random.default_rng(seed)
@@ -272,55 +273,71 @@ def star_layer_device(n: int, seed: int, nv_lo: int = 4, nv_hi: int = 4096, r_lo
     centre_xy = mixture_centres(rng, n) if centres == "mixture" else rng.random((n, 2))
     has_holes = rng.random(n) < hole_frac
     nholes = np.where(has_holes, rng.integers(1, 4, size=n), 0).astype(np.int64)
+    amp = rng.random((n, 5))
+    amp /= amp.sum(axis=1, keepdims=True)
+    phase = rng.uniform(0.0, 2.0 * np.pi, size=(n, 5))
+    hole_r = rng.uniform(0.3, 0.9, size=n)
+    # ring CSR on the host (one outer ring + holes per polygon)
+    rings_per_poly = 1 + nholes
+    poly_ring = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(rings_per_poly, out=poly_ring[1:])
+    n_rings = int(poly_ring[-1])
+    ring_poly = np.repeat(np.arange(n), rings_per_poly)
+    ring_j = np.arange(n_rings) - poly_ring[ring_poly]
+    hole_m = np.random.default_rng(seed + 7919).integers(3, 5, size=n_rings)
+    ring_nv = np.where(ring_j > 0, hole_m, nverts[ring_poly])
+    ring_vert = np.zeros(n_rings + 1, dtype=np.int64)
+    np.cumsum(ring_nv, out=ring_vert[1:])
+    total = int(ring_vert[-1])
+    dev = torch.device(device)
     g = torch.Generator(device=device)
     g.manual_seed(seed)
-    dev = torch.device(device)
-    nv = torch.from_numpy(nverts).to(dev)
-    rad = torch.from_numpy(radii).to(dev)
-    cen = torch.from_numpy(centre_xy).to(dev)
-    # rings: outer ring of polygon p, then its holes
-    rings_per_poly = torch.from_numpy(1 + nholes).to(dev)
-    poly_ring = torch.zeros(n + 1, dtype=torch.int64, device=dev)
-    torch.cumsum(rings_per_poly, 0, out=poly_ring[1:])
-    n_rings = int(poly_ring[-1])
-    ring_poly = torch.repeat_interleave(torch.arange(n, device=dev), rings_per_poly)
-    ring_j = torch.arange(n_rings, device=dev) - poly_ring[ring_poly]
-    is_hole = ring_j > 0
-    hole_m = torch.randint(3, 5, (n_rings,), generator=g, device=dev)
-    ring_nv = torch.where(is_hole, hole_m, nv[ring_poly])
-    ring_vert = torch.zeros(n_rings + 1, dtype=torch.int64, device=dev)
-    torch.cumsum(ring_nv, 0, out=ring_vert[1:])
-    total = int(ring_vert[-1])
-    owner_ring = torch.repeat_interleave(torch.arange(n_rings, device=dev), ring_nv)
-    k = torch.arange(total, device=dev) - ring_vert[owner_ring]
-    p = ring_poly[owner_ring]
-    hole_v = is_hole[owner_ring]
-    u = torch.rand(total, generator=g, device=dev, dtype=torch.float64)
-    # outer rings: jittered angle slots, radius r * U(0.5, 1), CCW
-    step = 2.0 * np.pi / nv[p].to(torch.float64)
-    theta = (k.to(torch.float64) + 0.1 + 0.8 * u) * step
-    jit = 0.5 + 0.5 * torch.rand(total, generator=g, device=dev, dtype=torch.float64)
-    amp = torch.from_numpy(rng.random((n, 5))).to(dev)
-    amp = amp / amp.sum(dim=1, keepdim=True)
-    phase = torch.from_numpy(rng.uniform(0.0, 2.0 * np.pi, size=(n, 5))).to(dev)
-    lobe = torch.zeros(total, dtype=torch.float64, device=dev)
-    for mm in range(5):
-        lobe += amp[p, mm] * torch.sin((mm + 1) * theta + phase[p, mm])
-    w = torch.from_numpy(_lobe_weight(nverts)).to(dev)[p]
-    rr = rad[p] * ((1.0 - w) * jit + w * (0.75 + 0.25 * lobe))
-    # holes: on a circle arc of their sector, descending angle (CW)
-    h = torch.from_numpy(nholes).to(dev)[p].clamp(min=1).to(torch.float64)
-    sector = 2.0 * np.pi / h
-    span = torch.clamp(sector, max=0.9 * np.pi)
-    a0 = sector * (ring_j[owner_ring] - 1).clamp(min=0).to(torch.float64) + 0.5 * (sector - span)
-    m = ring_nv[owner_ring].to(torch.float64)
-    frac = (m - 1 - k.to(torch.float64) + 0.5) / m  # evenly spaced, descending
-    hang = a0 + span * (0.15 + 0.7 * frac)
-    rin = 0.5 * torch.cos(torch.clamp(1.8 * np.pi / nv[p].clamp(min=4).to(torch.float64), max=1.45))
-    hr = (rad * torch.from_numpy(rng.uniform(0.3, 0.9, size=n)).to(dev))[p] * rin
-    ang = torch.where(hole_v, hang, theta)
-    r_all = torch.where(hole_v, hr, rr)
     xy = torch.empty((total, 2), dtype=torch.float64, device=dev)
-    xy[:, 0] = cen[p, 0] + r_all * torch.cos(ang)
-    xy[:, 1] = cen[p, 1] + r_all * torch.sin(ang)
-    return {"poly_ring": poly_ring, "ring_vert": ring_vert, "ring_hole": is_hole.to(torch.int32), "xy": xy}
+    lobe_w = _lobe_weight(nverts)
+    for c0 in range(0, n, chunk):
+        c1 = min(n, c0 + chunk)
+        r0, r1 = int(poly_ring[c0]), int(poly_ring[c1])
+        v0, v1 = int(ring_vert[r0]), int(ring_vert[r1])
+        t = lambda a, dt=None: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        rnv = t(ring_nv[r0:r1])
+        rpoly = t(ring_poly[r0:r1] - c0)
+        rj = t(ring_j[r0:r1])
+        rv = t(ring_vert[r0:r1] - v0)
+        m_v = v1 - v0
+        owner = torch.repeat_interleave(torch.arange(r1 - r0, device=dev), rnv)
+        k = torch.arange(m_v, device=dev) - rv[owner]
+        p = rpoly[owner]
+        hole_v = rj[owner] > 0
+        nv_p = t(nverts[c0:c1])[p].to(torch.float64)
+        u = torch.rand(m_v, generator=g, device=dev, dtype=torch.float64)
+        jit = 0.5 + 0.5 * torch.rand(m_v, generator=g, device=dev, dtype=torch.float64)
+        # outer rings: jittered angle slots, CCW, radius r * ((1-w) jitter + w lobes)
+        theta = (k.to(torch.float64) + 0.1 + 0.8 * u) * (2.0 * np.pi / nv_p)
+        A = t(amp[c0:c1])[p]
+        P = t(phase[c0:c1])[p]
+        lobe = torch.zeros(m_v, dtype=torch.float64, device=dev)
+        for mm in range(5):
+            lobe += A[:, mm] * torch.sin((mm + 1) * theta + P[:, mm])
+        del A, P
+        w = t(lobe_w[c0:c1])[p]
+        rad_p = t(radii[c0:c1])[p]
+        rr = rad_p * ((1.0 - w) * jit + w * (0.75 + 0.25 * lobe))
+        del lobe, w, jit, u
+        # holes: on a circle arc of their sector, descending angle (CW)
+        h = t(nholes[c0:c1])[p].clamp(min=1).to(torch.float64)
+        sector = 2.0 * np.pi / h
+        span = torch.clamp(sector, max=0.9 * np.pi)
+        a0 = sector * (rj[owner] - 1).clamp(min=0).to(torch.float64) + 0.5 * (sector - span)
+        m = rnv[owner].to(torch.float64)
+        frac = (m - 1 - k.to(torch.float64) + 0.5) / m
+        hang = a0 + span * (0.15 + 0.7 * frac)
+        rin = 0.5 * torch.cos(torch.clamp(1.8 * np.pi / nv_p.clamp(min=4), max=1.45))
+        hr = rad_p * t(hole_r[c0:c1])[p] * rin
+        ang = torch.where(hole_v, hang, theta)
+        r_all = torch.where(hole_v, hr, rr)
+        cen = t(centre_xy[c0:c1])[p]
+        xy[v0:v1, 0] = cen[:, 0] + r_all * torch.cos(ang)
+        xy[v0:v1, 1] = cen[:, 1] + r_all * torch.sin(ang)
+        del owner, k, p, hole_v, nv_p, theta, rr, h, sector, span, a0, m, frac, hang, rin, hr, ang, r_all, cen
+    return {"poly_ring": torch.from_numpy(poly_ring).to(dev), "ring_vert": torch.from_numpy(ring_vert).to(dev),
+            "ring_hole": torch.from_numpy((ring_j > 0).astype(np.int32)).to(dev), "xy": xy}
