@@ -302,6 +302,32 @@ int prt_pipeline_results(prt_pipeline *p, int64_t *h_pair_cont_off, int32_t *h_c
                          int32_t *h_cont_hole, double *h_xy);
 int prt_pipeline_free(prt_pipeline *p);
 
+/* ---------------------------------------------------------------- autotuner */
+
+/* Bounding box (x1, y1, x2, y2) of every polygon of a layer over all its
+ * rings, n_poly x 4 doubles into device memory (the MBRs the reference's
+ * readData quantises, vector_map_overlay_gpc_kernel.cu:752-888). */
+int prt_layer_mbr(const prt_layer *layer, double *d_out, void *stream);
+
+/* Autotuner (no reference counterpart): times the build + join for fanouts
+ * 8..32 and the batched clip for candidate schedules (warp-mode threshold,
+ * shared-memory slots, warps per SM) on an evenly strided sample of at most
+ * max_sample_pairs candidate pairs (<= 0: 200,000), within about
+ * time_budget_s seconds (<= 0: 30).  Installs the best schedule with
+ * prt_schedule_set and returns the choice. */
+typedef struct {
+  int32_t fanout;
+  int32_t candidates;      /* configurations timed */
+  int64_t sample_pairs;
+  double build_join_ms;    /* best build + join time (ms) */
+  double clip_ms;          /* best batched clip time on the sample (ms) */
+  double seconds;          /* tuning wall time */
+  prt_schedule sched;
+} prt_tuning;
+
+int prt_autotune(const prt_layer *base, const prt_layer *overlay, int op, int64_t max_sample_pairs,
+                 double time_budget_s, void *stream, prt_tuning *out);
+
 /* ---------------------------------------------------------------- area + adjoint */
 
 /* Intersection area of each pair (subject = base polygon pair_a[i], clip =

@@ -30,7 +30,7 @@ from ._lib import COORD, KEY, OP, SCHED, PrtError, check, lib
 __all__ = [
     "Tree", "Layer", "Results", "build_bottomup", "build_topdown", "overlay", "overlay_ref", "clip_pair",
     "intersection_area", "IntersectionArea", "PrtError", "device_count", "Pipeline", "get_schedule",
-    "set_schedule", "schedule",
+    "set_schedule", "schedule", "autotune",
 ]
 
 _DT2COORD = {torch.int64: COORD["i64"], torch.float32: COORD["f32"], torch.float64: COORD["f64"],
@@ -343,6 +343,56 @@ class schedule:
     def __exit__(self, *exc):
         set_schedule(self.prev)
         return False
+
+
+class _Tuning(C.Structure):
+    _fields_ = [("fanout", C.c_int32), ("candidates", C.c_int32), ("sample_pairs", C.c_int64),
+                ("build_join_ms", C.c_double), ("clip_ms", C.c_double), ("seconds", C.c_double),
+                ("sched", _Schedule)]
+
+
+def _tuning_cache_path(cache):
+    import os
+
+    if cache:
+        return cache
+    return os.environ.get("PRT_TUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "parlllelrtree_b200", "tuning.json"))
+
+
+def autotune(base: Layer, over: Layer, op: str = "int", max_sample_pairs: int = 200_000,
+             time_budget_s: float = 30.0, cache: str | None = None, use_cache: bool = True) -> dict:
+    """Chooses the tree fanout and the batched schedule for these layers
+    (prt_autotune: build + join timed per fanout, the batched clip timed per
+    candidate schedule on a strided sample of the candidate pairs) and
+    installs the schedule.  Results are cached in a JSON file keyed by the GPU
+    name and the layers' sizes; a cached entry is installed without timing."""
+    import json
+    import os
+
+    key = "|".join([torch.cuda.get_device_name(), op, str(base.n_poly), str(over.n_poly),
+                    str(int(base.ring_vert[-1])), str(int(over.ring_vert[-1]))])
+    path = _tuning_cache_path(cache)
+    db = {}
+    if use_cache and os.path.exists(path):
+        with open(path) as f:
+            db = json.load(f)
+        if key in db:
+            set_schedule(db[key]["schedule"])
+            return dict(db[key], cached=True)
+    t = _Tuning()
+    sb, so = base.struct(), over.struct()
+    check(lib().prt_autotune(C.byref(sb), C.byref(so), OP[op], int(max_sample_pairs), float(time_budget_s),
+                             _stream(), C.byref(t)))
+    res = {"fanout": int(t.fanout), "candidates": int(t.candidates), "sample_pairs": int(t.sample_pairs),
+           "build_join_ms": float(t.build_join_ms), "clip_ms": float(t.clip_ms), "seconds": float(t.seconds),
+           "schedule": t.sched.to_dict()}
+    if use_cache:
+        db[key] = res
+        os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+        with open(path, "w") as f:
+            json.dump(db, f, indent=1)
+    return dict(res, cached=False)
 
 
 class _PipelineConfig(C.Structure):

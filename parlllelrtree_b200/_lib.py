@@ -55,6 +55,8 @@ _SIGS = {
     "prt_clip_pair_host": (_I, [_I, _I, _P, _P, _I, _P, _P, _P, C.c_int32, _P, _P, _P, _I64, _P]),
     "prt_schedule_set": (_I, [_P]),
     "prt_schedule_get": (_I, [_P]),
+    "prt_layer_mbr": (_I, [_P, _P, _P]),
+    "prt_autotune": (_I, [_P, _P, _I, _I64, C.c_double, _P, _P]),
     "prt_pipeline_create": (_I, [_P, _P, _P, _P]),
     "prt_pipeline_run": (_I, [_P, _P]),
     "prt_pipeline_sizes": (_I, [_P, _P]),

@@ -658,7 +658,7 @@ __constant__ int8_t c_next_h[3][6] = {{BH, TH, TH, BH, NH, NH}, {NH, NH, NH, NH,
 // Clips subj against clip.  Returns the head of the output polygon list
 // (-1 for an empty result); read it with count_result / write_result /
 // result_area.  A.status != kClipOk means the arena was too small.
-static __device__ int clip_pair(Arena &A, int op, const PolyView &subj, const PolyView &clip) {
+static __device__ __noinline__ int clip_pair(Arena &A, int op, const PolyView &subj, const PolyView &clip) {
   const int sn = (int)(subj.r1 - subj.r0), cn = (int)(clip.r1 - clip.r0);
   if ((sn == 0 && cn == 0) || (sn == 0 && (op == OP_INT || op == OP_DIFF)) || (cn == 0 && op == OP_INT)) return -1;
 

@@ -70,7 +70,7 @@ __device__ inline bool resolve(const PairSrc &S, int64_t i, gpc::PolyView &a, gp
 
 // Records the clip result of pair i (arena A, output list head): per-pair
 // area, or contours and vertices reserved from the result pools.
-__device__ void finish_pair(const ClipOut &O, int64_t i, gpc::Arena &A, int head) {
+__device__ __noinline__ void finish_pair(const ClipOut &O, int64_t i, gpc::Arena &A, int head) {
   int nc = 0;
   int64_t nvt = 0;
   if (!A.status) gpc::count_result(A, head, &nc, &nvt);
@@ -109,7 +109,7 @@ __device__ inline void invalid_pair(const ClipOut &O, int64_t i) {
 }
 
 // One pair on the calling thread.
-__device__ void process_pair(const PairSrc &S, const ClipOut &O, int64_t i, unsigned char *slice, int scale) {
+__device__ __noinline__ void process_pair(const PairSrc &S, const ClipOut &O, int64_t i, unsigned char *slice, int scale) {
   gpc::PolyView a, b;
   int64_t nv = 0;
   if (!resolve(S, i, a, b, nv)) {
@@ -124,7 +124,7 @@ __device__ void process_pair(const PairSrc &S, const ClipOut &O, int64_t i, unsi
 
 // One pair on the calling warp (all lanes): the warp clipper, or the thread
 // clipper on lane 0 when the pair outgrows the warp's active-edge slots.
-__device__ void process_pair_warp(const PairSrc &S, const ClipOut &O, int64_t i, unsigned char *slice, int scale,
+__device__ __noinline__ void process_pair_warp(const PairSrc &S, const ClipOut &O, int64_t i, unsigned char *slice, int scale,
                                   gpc::WAet &W, unsigned long long *fallbacks) {
   const int lane = threadIdx.x & 31;
   gpc::PolyView a, b;
@@ -181,33 +181,37 @@ __global__ void __launch_bounds__(128) clip_plain_kernel(PairSrc S, ClipOut O, c
 // 32 in thread mode), then steals from the smaller bins after it.  One warp
 // per block spreads the big-pair warps over every SM; the block's dynamic
 // shared memory holds the warp clipper's active-edge slots.
-__global__ void __launch_bounds__(32) clip_lpt_kernel(PairSrc S, ClipOut O, const uint32_t *__restrict__ order,
-                                                      BinPlan plan, unsigned long long *tickets,
-                                                      unsigned char *arena, int scale,
-                                                      const int64_t *__restrict__ dyn_ranges) {
-  extern __shared__ __align__(16) unsigned char wsm[];
+__global__ void __launch_bounds__(32, 8) clip_lpt_kernel(PairSrc S, ClipOut O, const uint32_t *__restrict__ order,
+                                                         BinPlan plan, unsigned long long *tickets,
+                                                         unsigned char *arena, int scale,
+                                                         const int64_t *__restrict__ dyn_ranges) {
+  __shared__ int64_t s_begin[PRT_MAX_BINS], s_end[PRT_MAX_BINS];
+  __shared__ int32_t s_mode[PRT_MAX_BINS];
   const int lane = threadIdx.x & 31;
   const int64_t w = blockIdx.x;
-  if (dyn_ranges) {  // bin ranges computed on the device (graph mode)
-    for (int b = 0; b < plan.nbins; b++) {
-      plan.begin[b] = dyn_ranges[2 * b];
-      plan.end[b] = dyn_ranges[2 * b + 1];
-    }
+  const int nbins = plan.nbins;
+  if (lane < nbins) {
+    // bin ranges from the plan, or computed on the device (graph mode)
+    s_begin[lane] = dyn_ranges ? dyn_ranges[2 * lane] : plan.begin[lane];
+    s_end[lane] = dyn_ranges ? dyn_ranges[2 * lane + 1] : plan.end[lane];
+    s_mode[lane] = plan.warp_mode[lane];
   }
-  gpc::WAet W = gpc::waet_carve(wsm, plan.wcap);
+  __syncwarp();
+  gpc::WAet W = gpc::waet_carve(plan.wcap);
   int g = 0;
-  while (g + 1 < plan.nbins && w >= plan.warp0[g + 1]) g++;
+  while (g + 1 < nbins && w >= plan.warp0[g + 1]) g++;
   unsigned char *region = arena + plan.arena_off[g] + (w - plan.warp0[g]) * plan.region[g];
   unsigned char *slice = region + (int64_t)lane * ((plan.region[g] / 32) & ~(int64_t)15);
   unsigned long long *fallbacks = tickets + PRT_MAX_BINS;
-  for (int b = g; b < plan.nbins; b++) {
-    if (plan.warp_mode[b]) {
+  for (int b = g; b < nbins; b++) {
+    const int64_t begin = s_begin[b], end = s_end[b];
+    if (s_mode[b]) {
       for (;;) {
         unsigned long long t = 0;
         if (lane == 0) t = atomicAdd(&tickets[b], 1ull);
         t = __shfl_sync(0xffffffffu, t, 0);
-        const int64_t k = plan.begin[b] + (int64_t)t;
-        if (k >= plan.end[b]) break;
+        const int64_t k = begin + (int64_t)t;
+        if (k >= end) break;
         process_pair_warp(S, O, (int64_t)order[k], region, scale, W, fallbacks);
       }
     } else {
@@ -215,10 +219,10 @@ __global__ void __launch_bounds__(32) clip_lpt_kernel(PairSrc S, ClipOut O, cons
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(&tickets[b], 32ull);
         base = __shfl_sync(0xffffffffu, base, 0);
-        const int64_t k0 = plan.begin[b] + (int64_t)base;
-        if (k0 >= plan.end[b]) break;
+        const int64_t k0 = begin + (int64_t)base;
+        if (k0 >= end) break;
         const int64_t k = k0 + lane;
-        if (k < plan.end[b]) process_pair(S, O, (int64_t)order[k], slice, scale);
+        if (k < end) process_pair(S, O, (int64_t)order[k], slice, scale);
         __syncwarp();
       }
     }
@@ -254,10 +258,12 @@ __global__ void bin_bounds_kernel(const uint32_t *__restrict__ k0, const uint32_
   maxnv[b] = lo < n ? (int64_t)(0xFFFFFFFFu - k[lo]) : 0;
 }
 
-__global__ void select_u32_kernel(const uint32_t *a, const uint32_t *b, const int *sel, int64_t n, uint32_t *dst) {
+// dst[i] = the sorted value i (from a or b per *sel), mapped through idx when given.
+__global__ void select_u32_kernel(const uint32_t *a, const uint32_t *b, const int *sel, int64_t n, uint32_t *dst,
+                                  const int64_t *__restrict__ idx = nullptr) {
   const uint32_t *src = *sel ? b : a;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    dst[i] = src[i];
+    dst[i] = idx ? (uint32_t)idx[src[i]] : src[i];
 }
 
 __global__ void area_from_results_kernel(const int64_t *__restrict__ pair_cstart, const int32_t *__restrict__ pair_ncont,
@@ -322,16 +328,16 @@ size_t arena_budget() {
 
 // ---- batched schedule ----------------------------------------------------------
 // Default: pairs above 256 vertices are clipped one per warp, smaller ones one
-// per thread; the warps per SM of all bins add up to what the SM holds at the
-// default slot count.
+// per thread; the warps per SM of all bins add up to the 8 warps an SM holds
+// at the clip kernel's register count.
 static prt_schedule default_schedule() {
   prt_schedule d;
   memset(&d, 0, sizeof d);
   d.nbins = 5;
-  d.aet_slots = 256;
+  d.aet_slots = 128;
   const int64_t thr[5] = {1ll << 40, 4096, 1024, 256, 64};
   const int32_t wm[5] = {1, 1, 1, 0, 0};
-  const int32_t wps[5] = {4, 3, 3, 2, 2};
+  const int32_t wps[5] = {2, 2, 2, 1, 1};
   for (int b = 0; b < 5; b++) {
     d.bin_thresholds[b] = thr[b];
     d.bin_warp_mode[b] = wm[b];
@@ -366,15 +372,16 @@ int schedule_valid(const prt_schedule &s) {
 }
 
 size_t plan_bins(const prt_schedule &sc, const int64_t *counts, const int64_t *maxnv, size_t budget, BinPlan &plan,
-                 size_t *smem) {
+                 size_t *smem, int scale) {
   memset(&plan, 0, sizeof plan);
   plan.nbins = sc.nbins;
   plan.wcap = sc.aet_slots;
   int64_t need[PRT_MAX_BINS];
   bool any_warp = false;
   for (int b = 0; b < sc.nbins; b++) {
-    const int64_t sl = (int64_t)gpc::align16(gpc::arena_bytes(gpc::caps_for(maxnv[b] > 0 ? maxnv[b] : 4, 1)));
+    const gpc::Caps caps = gpc::caps_for(maxnv[b] > 0 ? maxnv[b] : 4, scale);
     plan.warp_mode[b] = sc.bin_warp_mode[b];
+    const int64_t sl = (int64_t)gpc::align16(sc.bin_warp_mode[b] ? gpc::warp_arena_bytes(caps) : gpc::arena_bytes(caps));
     need[b] = counts[b] > 0 ? (sc.bin_warp_mode[b] ? sl : 32 * sl) : 0;
     any_warp |= sc.bin_warp_mode[b] && counts[b] > 0;
   }
@@ -406,6 +413,7 @@ struct OverlayState {
   PairSrc S;
   ClipOut O;
   int64_t n;
+  int sched = PRT_SCHED_PLAIN;
   int64_t retried = 0;
 };
 
@@ -519,8 +527,11 @@ int prepare_lpt_launch(size_t smem) {
   return PRT_OK;
 }
 
-static int run_batched(OverlayState &st, cudaStream_t s) {
-  const int64_t n = st.n;
+// Batched launch over items [0, count) of idx (or all pairs when idx is NULL)
+// with arena slices of `scale` times the first size.
+static int run_batched(OverlayState &st, const int64_t *d_idx, int64_t count, int scale, cudaStream_t s) {
+  if (count == 0) return PRT_OK;
+  const int64_t n = count;
   const prt_schedule sc = current_schedule();
   const int nb = sc.nbins;
   int64_t *nv = nullptr;
@@ -544,7 +555,7 @@ static int run_batched(OverlayState &st, cudaStream_t s) {
   const int g = grid_for(n, 256, 16);
   {
     PRT_PROF("nv", s);
-    nv_kernel<<<g, 256, 0, s>>>(st.S, n, nullptr, 1, nv, nullptr);
+    nv_kernel<<<g, 256, 0, s>>>(st.S, n, d_idx, 1, nv, nullptr);
   }
   {
     PRT_PROF("size_key", s);
@@ -555,7 +566,7 @@ static int run_batched(OverlayState &st, cudaStream_t s) {
   if (!rc) {
     {
       PRT_PROF("select_u32", s);
-      select_u32_kernel<<<g, 256, 0, s>>>(v0, v1, sel, n, order);
+      select_u32_kernel<<<g, 256, 0, s>>>(v0, v1, sel, n, order, d_idx);
     }
     {
       PRT_PROF("bin_bounds", s);
@@ -572,7 +583,7 @@ static int run_batched(OverlayState &st, cudaStream_t s) {
   int64_t counts[PRT_MAX_BINS];
   for (int b = 0; b < nb; b++) counts[b] = hb[b + 1] - hb[b];
   size_t smem = 0;
-  const size_t bytes = plan_bins(sc, counts, hm, arena_budget(), plan, &smem);
+  const size_t bytes = plan_bins(sc, counts, hm, arena_budget(), plan, &smem, scale);
   for (int b = 0; b < nb; b++) {
     plan.begin[b] = hb[b];
     plan.end[b] = hb[b + 1];
@@ -583,7 +594,7 @@ static int run_batched(OverlayState &st, cudaStream_t s) {
   if (!rc && warps > 0) rc = dmalloc(reinterpret_cast<void **>(&arena), bytes, s);
   if (!rc && warps > 0) {
     PRT_PROF("clip_batched", s);
-    clip_lpt_kernel<<<(unsigned)warps, 32, smem, s>>>(st.S, st.O, order, plan, tickets, arena, 1, nullptr);
+    clip_lpt_kernel<<<(unsigned)warps, 32, smem, s>>>(st.S, st.O, order, plan, tickets, arena, scale, nullptr);
   }
   if (!rc) {
     cudaError_t e = cudaGetLastError();
@@ -655,7 +666,8 @@ static int retry_failed(OverlayState &st, cudaStream_t s) {
       int rc = dalloc(&d_idx, idx.size(), s);
       if (rc) return rc;
       cudaMemcpyAsync(d_idx, idx.data(), 8 * idx.size(), cudaMemcpyHostToDevice, s);
-      rc = run_plain(st, d_idx, (int64_t)idx.size(), sc, s);
+      rc = st.sched == PRT_SCHED_PLAIN ? run_plain(st, d_idx, (int64_t)idx.size(), sc, s)
+                                       : run_batched(st, d_idx, (int64_t)idx.size(), sc, s);
       dfree(d_idx, s);
       if (rc) return rc;
     }
@@ -823,6 +835,7 @@ int overlay_impl(const PairSrc &S, int64_t n, int sched, double *d_area, cudaStr
   OverlayState st;
   st.S = S;
   st.n = n;
+  st.sched = sched;
   memset(&st.O, 0, sizeof st.O);
   st.O.area = d_area;
   int rc = dalloc(&st.O.status, std::max<int64_t>(n, 1), s);
@@ -850,10 +863,10 @@ int overlay_impl(const PairSrc &S, int64_t n, int sched, double *d_area, cudaStr
     dfree(tmp, s);
   }
   if (!rc && !d_area) {
-    // first guess at the result size (grown on demand): a quarter of the input
+    // first guess at the result size (grown on demand): half of the input
     // vertices, one contour per 64 of them
     st.O.cap_c = total_nv / 64 + 1024;
-    st.O.cap_v = total_nv / 4 + 4096;
+    st.O.cap_v = total_nv / 2 + 4096;
     rc = dalloc(&st.O.cont_vstart, st.O.cap_c, s);
     if (!rc) rc = dalloc(&st.O.cont_nverts, st.O.cap_c, s);
     if (!rc) rc = dalloc(&st.O.cont_hole, st.O.cap_c, s);
@@ -864,7 +877,7 @@ int overlay_impl(const PairSrc &S, int64_t n, int sched, double *d_area, cudaStr
     if (e == cudaSuccess) e = cudaMemsetAsync(st.O.status, 0, 4 * std::max<int64_t>(n, 1), s);
     if (e != cudaSuccess) rc = cuda_status(e, "memset");
   }
-  if (!rc && n > 0) rc = sched == PRT_SCHED_PLAIN ? run_plain(st, nullptr, n, 1, s) : run_batched(st, s);
+  if (!rc && n > 0) rc = sched == PRT_SCHED_PLAIN ? run_plain(st, nullptr, n, 1, s) : run_batched(st, nullptr, n, 1, s);
   if (!rc && n > 0) rc = retry_failed(st, s);
   if (rc || d_area) {
     if (!rc) {

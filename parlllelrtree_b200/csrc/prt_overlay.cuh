@@ -68,7 +68,7 @@ int schedule_valid(const prt_schedule &s);
 // vertices, arena limited to `budget` bytes; returns the arena bytes and the
 // dynamic shared memory per block in *smem.
 size_t plan_bins(const prt_schedule &sc, const int64_t *counts, const int64_t *maxnv, size_t budget, BinPlan &plan,
-                 size_t *smem);
+                 size_t *smem, int scale = 1);
 
 // Allows the persistent clip kernel `smem` bytes of dynamic shared memory.
 int prepare_lpt_launch(size_t smem);

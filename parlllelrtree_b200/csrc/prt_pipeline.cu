@@ -154,6 +154,15 @@ int prt_pipeline_create(const prt_layer *base, const prt_layer *overlay, const p
     if (rs) return rs;
   }
   cfg.sched = nullptr;  // the pipeline keeps its own copy in the plan
+  {
+    // memory cached by the stream-ordered pool goes back to the device first
+    cudaMemPool_t pool;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceSynchronize() == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
+      cudaMemPoolTrimTo(pool, 0);
+    cudaGetLastError();
+  }
   prt_pipeline *p = new prt_pipeline();
   p->cfg = cfg;
   p->base = layer_dev(base);
@@ -241,6 +250,19 @@ int prt_pipeline_create(const prt_layer *base, const prt_layer *overlay, const p
     return rc;
   }
   *out = p;
+  return PRT_OK;
+}
+
+int prt_layer_mbr(const prt_layer *layer, double *d_out, void *stream) {
+  PRT_CHECK(layer && d_out, PRT_ERR_INVALID, "NULL argument");
+  PRT_CHECK(layer->n_poly >= 0, PRT_ERR_INVALID, "n_poly %lld", (long long)layer->n_poly);
+  if (layer->n_poly == 0) return PRT_OK;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  {
+    PRT_PROF("poly_mbr", s);
+    poly_mbr_kernel<<<grid_for(layer->n_poly, 256, 8), 256, 0, s>>>(layer_dev(layer), d_out);
+  }
+  PRT_CUDA(cudaGetLastError());
   return PRT_OK;
 }
 

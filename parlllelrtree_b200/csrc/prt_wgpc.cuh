@@ -8,28 +8,33 @@
 // vertices that is a chain of dependent loads per edge per pass.  Here the AET
 // is an ARRAY of slots in shared memory, in AET order, and every per-beam pass
 // is data-parallel over the slots:
-//   insertion of the beam's local minima   ballot for the insertion point, shift
-//   bundle detection (GPC:371-393)          segmented XOR scan over the edges
-//                                           that do not end at yb
-//   parity and horizontal state (GPC:395-423) XOR scans and a scan of the
-//                                           3-state transition functions
-//   vertex classes                          per slot from the scanned state
-//   output (GPC:425-570)                    lane 0, only for contributing slots,
-//                                           in AET order (the output lists are
-//                                           the reference's linked structure)
-//   deletion of terminating edges, xt       ballot compaction
-//   intersection test (GPC:461-485)         fast check that the ST insertion
-//                                           would record no intersection; a beam
-//                                           that has intersections spills the
-//                                           slots to the linked form and runs the
-//                                           thread clipper's intersect_beam
-//   successor edges (GPC:661-693)           per slot
-// The build phase (local-minima table, scanbeam table) is parallel too: ring
-// staging by ballot, bound edges written by the whole warp, stable warp radix
-// sorts instead of the heap sort.  Any case the slot array cannot hold (more
-// active edges than slots, an AET list the intersection step left malformed,
-// more rings than the ring scratch holds) makes the caller rerun the pair with
-// the thread clipper, so the result is always the thread clipper's.
+//   insertion of the beam's local minima    ballot for the insertion point, shift
+//   bundle detection (GPC:371-393)           segmented XOR over the edges that
+//                                            do not end at yb
+//   parity and horizontal state (GPC:395-423) popcounts of ballots (the state
+//                                            changes only at one-sided edges)
+//   vertex classes                           per slot from that state
+//   output (GPC:425-570)                     continuing edges in parallel; the
+//                                            events (vertices, local minima and
+//                                            maxima) on lane 0 in AET order; a
+//                                            contour merge's redirect by the warp
+//   next scanbeam, deletion, xt (GPC:426-459) warp min and ballot compaction
+//   intersection test (GPC:461-485)          fast check that the ST insertion
+//                                            would record no intersection; a beam
+//                                            that has intersections spills the
+//                                            slots to the linked form and runs the
+//                                            thread clipper's intersect_beam
+//   successor edges (GPC:661-693)            per slot
+// The build is parallel too: ring staging by ballot, bound edges written by
+// the whole warp, the local-minima table sorted by a stable warp radix sort.
+// No scanbeam table is sorted: every vertex y is a local minimum or the top
+// of an edge, so the next beam is the lower of the next local minimum and the
+// lowest top of an active edge, which walks the same sorted unique ys as
+// GPC's table (build_sbt, GPC:1019-1085).  An active edge table larger than
+// the shared-memory slots moves to the pair's arena; only an AET list the
+// intersection step leaves malformed or more rings than the ring scratch
+// holds make the caller rerun the pair with the thread clipper, so the result
+// is always the thread clipper's.
 #pragma once
 #include "prt_gpc.cuh"
 
@@ -37,80 +42,126 @@ namespace prt {
 namespace gpc {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr double kInf = __builtin_huge_val();
 
 // Slot flag bits.
 enum : uint32_t {
-  W_TYPE = 1u,             // SUBJ edge
-  W_BA = 1,                // bits 1-2: bundle[ABOVE][CLIP], [SUBJ]
-  W_BB = 3,                // bits 3-4: bundle[BELOW]
-  W_SIDE = 5,              // bits 5-6: bside[CLIP], bside[SUBJ]
-  W_STA = 7,               // bits 7-8: bstate[ABOVE]
-  W_STB = 9,               // bits 9-10: bstate[BELOW]
-  W_VC = 11,               // bits 11-14: vertex class
+  W_TYPE = 1u,         // SUBJ edge
+  W_BA = 1,            // bits 1-2: bundle[ABOVE][CLIP], [SUBJ]
+  W_BB = 3,            // bits 3-4: bundle[BELOW]
+  W_SIDE = 5,          // bits 5-6: bside[CLIP], bside[SUBJ]
+  W_STA = 7,           // bits 7-8: bstate[ABOVE]
+  W_STB = 9,           // bits 9-10: bstate[BELOW]
+  W_VC = 11,           // bits 11-14: vertex class
   W_CONTRIB = 1u << 15,
-  W_STARTS = 1u << 16,     // the edge starts at yb
+  W_STARTS = 1u << 16,  // the edge starts at yb
+  W_PXNE = 1u << 17,    // xb differs from GPC's px (the x of the last output event before it)
 };
 
 __device__ inline int fbits(uint32_t f, int sh) { return (int)((f >> sh) & 3u); }
 __device__ inline uint32_t fset(uint32_t f, int sh, int v) { return (f & ~(3u << sh)) | ((uint32_t)v << sh); }
 
 struct WSlot {
-  double xb, xt, dx, ty;
-  int32_t edge, outA, outB;
+  double xb, xt, dx, ty, bx, by, tx;
+  int32_t edge, outA, outB, succ;
   uint32_t fl;
 };
 
-// Shared-memory slot arrays of one warp (structure of arrays).
+// Dynamic shared memory of the block (one warp per block): the warp
+// clipper's slot arrays, then the radix counters and the cached output
+// polygon nodes.
+extern __shared__ __align__(16) unsigned char prt_wsm[];
+
+// Output polygon nodes kept in shared memory per warp.
+constexpr int kWarpPolyNodes = 128;
+
+// Bytes of the slot arrays for cap slots: 7 double arrays, 6 int arrays,
+// cap/32 event masks.
+__host__ __device__ inline size_t wslot_bytes(int cap) {
+  return (size_t)cap * (7 * 8 + 6 * 4) + (size_t)(cap / 32) * 4;
+}
+
+// Dynamic shared memory per warp: slots, 256 radix counters, polygon nodes.
+__host__ __device__ inline size_t waet_bytes(int cap) {
+  return wslot_bytes(cap) + 256 * 4 + sizeof(PolyNode) * kWarpPolyNodes;
+}
+
+// Arena of one pair in warp mode: the thread clipper's arena, then room for
+// an active edge table as large as the pair's edge count, where the slots go
+// when they outgrow shared memory.
+__host__ __device__ inline size_t warp_arena_bytes(const Caps &c) {
+  return arena_bytes(c) + align16(wslot_bytes((c.e + 31) / 32 * 32));
+}
+
+// Slot arrays of one warp (structure of arrays): the dynamic state of each
+// active edge and the static fields every beam reads (bottom, top x,
+// successor), so no pass over the slots reads the edge table.  `base` is the
+// block's shared memory until the table outgrows it, then the arena.
 struct WAet {
-  double *xb, *xt, *dx, *ty;
-  int32_t *edge, *outA, *outB, *ord;
-  uint32_t *fl;
-  uint32_t *cnt;  // 256 radix counters
-  int cap;
+  unsigned char *base;
+  int cap;     // slots at base
+  int scap;    // slots of the shared-memory layout (fixed at launch)
+  int spcap;   // polygon nodes in shared memory
+  __device__ double *dbl(int k) const { return reinterpret_cast<double *>(base) + k * cap; }
+  __device__ int32_t *i32(int k) const { return reinterpret_cast<int32_t *>(base + 56 * (size_t)cap) + k * cap; }
+  __device__ double *xb() const { return dbl(0); }
+  __device__ double *xt() const { return dbl(1); }
+  __device__ double *dx() const { return dbl(2); }
+  __device__ double *ty() const { return dbl(3); }
+  __device__ double *bx() const { return dbl(4); }
+  __device__ double *by() const { return dbl(5); }
+  __device__ double *tx() const { return dbl(6); }
+  __device__ int32_t *edge() const { return i32(0); }
+  __device__ int32_t *outA() const { return i32(1); }
+  __device__ int32_t *outB() const { return i32(2); }
+  __device__ int32_t *succ() const { return i32(3); }
+  __device__ int32_t *ord() const { return i32(4); }
+  __device__ uint32_t *fl() const { return reinterpret_cast<uint32_t *>(i32(5)); }
+  __device__ uint32_t *cmask() const { return reinterpret_cast<uint32_t *>(i32(6)); }
 };
 
-__host__ __device__ inline size_t waet_bytes(int cap) { return (size_t)cap * (4 * 8 + 5 * 4) + 256 * 4; }
+__device__ inline uint32_t *wsm_counters(int scap) { return reinterpret_cast<uint32_t *>(prt_wsm + wslot_bytes(scap)); }
+__device__ inline PolyNode *wsm_polys(int scap) { return reinterpret_cast<PolyNode *>(wsm_counters(scap) + 256); }
 
-__device__ inline WAet waet_carve(unsigned char *smem, int cap) {
+__device__ inline WAet waet_carve(int cap) {
   WAet w;
+  w.base = prt_wsm;
   w.cap = cap;
-  double *d = reinterpret_cast<double *>(smem);
-  w.xb = d;
-  w.xt = d + cap;
-  w.dx = d + 2 * cap;
-  w.ty = d + 3 * cap;
-  int32_t *i = reinterpret_cast<int32_t *>(d + 4 * cap);
-  w.edge = i;
-  w.outA = i + cap;
-  w.outB = i + 2 * cap;
-  w.ord = i + 3 * cap;
-  w.fl = reinterpret_cast<uint32_t *>(i + 4 * cap);
-  w.cnt = w.fl + cap;
+  w.scap = cap;
+  w.spcap = kWarpPolyNodes;
   return w;
 }
 
 __device__ inline WSlot wload(const WAet &w, int s) {
   WSlot v;
-  v.xb = w.xb[s];
-  v.xt = w.xt[s];
-  v.dx = w.dx[s];
-  v.ty = w.ty[s];
-  v.edge = w.edge[s];
-  v.outA = w.outA[s];
-  v.outB = w.outB[s];
-  v.fl = w.fl[s];
+  v.xb = w.xb()[s];
+  v.xt = w.xt()[s];
+  v.dx = w.dx()[s];
+  v.ty = w.ty()[s];
+  v.bx = w.bx()[s];
+  v.by = w.by()[s];
+  v.tx = w.tx()[s];
+  v.edge = w.edge()[s];
+  v.outA = w.outA()[s];
+  v.outB = w.outB()[s];
+  v.succ = w.succ()[s];
+  v.fl = w.fl()[s];
   return v;
 }
 
 __device__ inline void wstore(const WAet &w, int s, const WSlot &v) {
-  w.xb[s] = v.xb;
-  w.xt[s] = v.xt;
-  w.dx[s] = v.dx;
-  w.ty[s] = v.ty;
-  w.edge[s] = v.edge;
-  w.outA[s] = v.outA;
-  w.outB[s] = v.outB;
-  w.fl[s] = v.fl;
+  w.xb()[s] = v.xb;
+  w.xt()[s] = v.xt;
+  w.dx()[s] = v.dx;
+  w.ty()[s] = v.ty;
+  w.bx()[s] = v.bx;
+  w.by()[s] = v.by;
+  w.tx()[s] = v.tx;
+  w.edge()[s] = v.edge;
+  w.outA()[s] = v.outA;
+  w.outB()[s] = v.outB;
+  w.succ()[s] = v.succ;
+  w.fl()[s] = v.fl;
 }
 
 // A slot holding edge e with the edge's stored state.
@@ -122,6 +173,10 @@ __device__ inline WSlot wslot_of(const Arena &A, int e) {
   v.xt = E.xt;
   v.dx = E.dx;
   v.ty = E.ty;
+  v.bx = E.bx;
+  v.by = E.by;
+  v.tx = E.tx;
+  v.succ = E.succ;
   v.outA = E.outp[ABOVE];
   v.outB = E.outp[BELOW];
   v.fl = (E.type ? W_TYPE : 0u) | ((uint32_t)(E.bundle[ABOVE][CLIP] | (E.bundle[ABOVE][SUBJ] << 1)) << W_BA) |
@@ -229,8 +284,8 @@ __device__ inline void warp_copy(T *dst, const T *src, int n) {
 // ---------------------------------------------------------------- build
 // Bounds of ring r (build_lmt, GPC:1175-1307) with the whole warp: the optimal
 // vertices are staged by ballot, each local minimum's bound is measured by a
-// warp-wide walk and its edges are written in parallel.  Edges, bounds and
-// scanbeam entries come out in the thread clipper's order.
+// warp-wide walk and its edges are written in parallel.  Edges and bounds
+// come out in the thread clipper's order.
 __device__ inline void wbuild_ring(Arena &A, const PolyView &p, int64_t r, int type, int op, double *sx,
                                    double *sy) {
   const int lane = threadIdx.x & 31;
@@ -253,18 +308,9 @@ __device__ inline void wbuild_ring(Arena &A, const PolyView &p, int64_t r, int t
       const int kk = k + __popc(m & lanemask_lt());
       sx[kk] = x;
       sy[kk] = y;
-      if (A.ny + kk < A.cap.y) {
-        A.Y[A.ny + kk].y = y;
-        A.Y[A.ny + kk].order = A.ny + kk;
-      }
     }
     k += __popc(m);
   }
-  if (A.ny + k > A.cap.y) {
-    A.status = kClipCapacity;
-    return;
-  }
-  A.ny += k;
   __syncwarp();
   for (int dir = 0; dir < 2; dir++) {
     for (int c = 0; c < k; c += 32) {
@@ -333,10 +379,10 @@ __device__ inline void wbuild_ring(Arena &A, const PolyView &p, int64_t r, int t
   __syncwarp();
 }
 
-// Ring contributions (minimax_test, GPC:1656-1709) and all bounds; then the
-// sorted local-minima table and the sorted unique scanbeam table.  Returns
-// false when the pair has more rings than the ring scratch holds.
-__device__ inline bool wbuild(Arena &A, int op, const PolyView &subj, const PolyView &clip, WAet &W, int *nsbt) {
+// Ring contributions (minimax_test, GPC:1656-1709), all bounds, and the
+// sorted local-minima table.  Returns false when the pair has more rings
+// than the ring scratch holds.
+__device__ inline bool wbuild(Arena &A, int op, const PolyView &subj, const PolyView &clip, const WAet &W) {
   const int lane = threadIdx.x & 31;
   const int sn = (int)(subj.r1 - subj.r0), cn = (int)(clip.r1 - clip.r0);
   const bool minimax = (op == OP_INT || op == OP_DIFF) && sn > 0 && cn > 0;
@@ -398,48 +444,30 @@ __device__ inline bool wbuild(Arena &A, int op, const PolyView &subj, const Poly
   if (A.status || A.nb == 0) return true;
   // local-minima table: (y, x, dx), ties in creation order = three stable
   // passes, least significant key first
+  uint32_t *cnt = wsm_counters(W.scap);
   Bound *bs = reinterpret_cast<Bound *>(A.IT);
-  Bound *cur = warp_radix(A.B, bs, A.nb, [](const Bound &b) { return dkey(b.dx); }, W.cnt);
+  Bound *cur = warp_radix(A.B, bs, A.nb, [](const Bound &b) { return dkey(b.dx); }, cnt);
   Bound *oth = cur == A.B ? bs : A.B;
-  cur = warp_radix(cur, oth, A.nb, [](const Bound &b) { return dkey(b.x); }, W.cnt);
+  cur = warp_radix(cur, oth, A.nb, [](const Bound &b) { return dkey(b.x); }, cnt);
   oth = cur == A.B ? bs : A.B;
-  cur = warp_radix(cur, oth, A.nb, [](const Bound &b) { return dkey(b.y); }, W.cnt);
+  cur = warp_radix(cur, oth, A.nb, [](const Bound &b) { return dkey(b.y); }, cnt);
   if (cur != A.B) warp_copy(A.B, cur, A.nb);
-  YKey *ys = reinterpret_cast<YKey *>(A.ST);
-  YKey *yc = warp_radix(A.Y, ys, A.ny, [](const YKey &k) { return dkey(k.y); }, W.cnt);
-  if (yc != A.Y) warp_copy(A.Y, yc, A.ny);
-  // unique y, compacted in place
-  int cnt = 0;
-  double last = 0.0;
-  for (int c = 0; c < A.ny; c += 32) {
-    const int i = c + lane;
-    double y = 0.0, prev = 0.0;
-    if (i < A.ny) y = A.Y[i].y;
-    prev = __shfl_up_sync(kFull, y, 1);
-    if (lane == 0) prev = last;
-    const bool keep = i < A.ny && (i == 0 || y > prev);
-    const unsigned m = __ballot_sync(kFull, keep);
-    last = __shfl_sync(kFull, y, 31);
-    __syncwarp();
-    if (keep) A.Y[cnt + __popc(m & lanemask_lt())].y = y;
-    cnt += __popc(m);
-    __syncwarp();
-  }
-  *nsbt = cnt;
   return true;
 }
 
-__constant__ int8_t c_wnext_h[3][6] = {{BH, TH, TH, BH, NH, NH}, {NH, NH, NH, NH, TH, TH}, {NH, NH, NH, NH, BH, BH}};
+// ---------------------------------------------------------------- output polygons
+// Output polygon nodes of the warp clipper: node k lives in shared memory
+// when k < spcap, else in the arena.  The functions below are the thread
+// clipper's add_local_min / add_left / add_right / merge_* (GPC:1506-1621)
+// over this split store.
+struct WPoly {
+  PolyNode *sp;
+  PolyNode *gp;
+  int spcap;
+  __device__ PolyNode &operator[](int k) const { return k < spcap ? sp[k] : gp[k]; }
+};
 
-// 3-state transition function packed as 2 bits per state.
-__device__ inline uint32_t hf_apply(uint32_t f, int h) { return (f >> (2 * h)) & 3u; }
-__device__ inline uint32_t hf_compose(uint32_t later, uint32_t earlier) {  // later(earlier(h))
-  return hf_apply(later, (int)hf_apply(earlier, 0)) | (hf_apply(later, (int)hf_apply(earlier, 1)) << 2) |
-         (hf_apply(later, (int)hf_apply(earlier, 2)) << 4);
-}
-constexpr uint32_t kHfIdentity = 0u | (1u << 2) | (2u << 4);
-
-__device__ inline int w_add_local_min(Arena &A, int &out_poly, double x, double y) {
+__device__ inline int wp_local_min(Arena &A, const WPoly &P, int &out_poly, double x, double y) {
   if (A.np >= A.cap.p) {
     A.status = kClipCapacity;
     return -1;
@@ -447,7 +475,7 @@ __device__ inline int w_add_local_min(Arena &A, int &out_poly, double x, double 
   int v = new_vertex(A, x, y, -1);
   if (v < 0) return -1;
   int k = A.np++;
-  PolyNode &p = A.P[k];
+  PolyNode &p = P[k];
   p.active = 1;
   p.hole = 0;
   p.next = out_poly;
@@ -458,41 +486,152 @@ __device__ inline int w_add_local_min(Arena &A, int &out_poly, double x, double 
   return k;
 }
 
+__device__ inline void wp_add_left(Arena &A, const WPoly &P, int p, double x, double y) {
+  if (p < 0) return;
+  PolyNode &q = P[P[p].proxy];
+  int v = new_vertex(A, x, y, q.vl);
+  if (v >= 0) q.vl = v;
+}
+
+__device__ inline void wp_add_right(Arena &A, const WPoly &P, int p, double x, double y) {
+  if (p < 0) return;
+  PolyNode &q = P[P[p].proxy];
+  int v = new_vertex(A, x, y, -1);
+  if (v < 0) return;
+  A.V[q.vr].next = v;
+  q.vr = v;
+}
+
+// merge_left / merge_right without the redirect: returns the proxy to
+// redirect (*to receives its replacement), or -1.  The redirect itself
+// (every node whose proxy is the old one becomes inactive and takes the new
+// one) touches every node of the output list, which holds all nodes ever
+// created (nodes are only prepended); the warp does it as one parallel pass
+// over the node array (wp_redirect_all), in any order, as the update is the
+// same for every node.
+__device__ inline int wp_merge_left(Arena &A, const WPoly &P, int p, int q, int *to) {
+  if (p < 0 || q < 0) return -1;
+  int pp = P[p].proxy, qp = P[q].proxy;
+  P[qp].hole = 1;
+  if (pp == qp) return -1;
+  A.V[P[pp].vr].next = P[qp].vl;
+  P[qp].vl = P[pp].vl;
+  *to = qp;
+  return pp;
+}
+
+__device__ inline int wp_merge_right(Arena &A, const WPoly &P, int p, int q, int *to) {
+  if (p < 0 || q < 0) return -1;
+  int pp = P[p].proxy, qp = P[q].proxy;
+  P[qp].hole = 0;
+  if (pp == qp) return -1;
+  A.V[P[qp].vr].next = P[pp].vl;
+  P[qp].vr = P[pp].vr;
+  *to = qp;
+  return pp;
+}
+
+// All lanes: nodes [0, np) whose proxy is `target` become inactive and point
+// at `to` (redirect, GPC:1529-1540 / 1574-1585).
+__device__ inline void wp_redirect_all(const WPoly &P, int np, int target, int to) {
+  for (int k = threadIdx.x & 31; k < np; k += 32) {
+    PolyNode &n = P[k];
+    if (n.proxy == target) {
+      n.active = 0;
+      n.proxy = to;
+    }
+  }
+  __syncwarp();
+}
+
+// Copies the shared-memory nodes to the arena (dir 0) or back (dir 1); np
+// is lane 0's count.
+__device__ inline void wp_sync(const WPoly &P, int np, int dir) {
+  np = __shfl_sync(kFull, np, 0);
+  const int m = np < P.spcap ? np : P.spcap;
+  for (int k = threadIdx.x & 31; k < m; k += 32) {
+    if (dir == 0) P.gp[k] = P.sp[k];
+    else P.sp[k] = P.gp[k];
+  }
+  __syncwarp();
+}
+
 enum : int { kWarpOk = 0, kWarpFallback = 1 };
 
-// Clips subj against clip with the calling warp (all 32 lanes, converged).
-// Returns the output polygon list head on every lane; A.status and the
-// output counters are valid on every lane.  *mode = kWarpFallback when the
-// pair needs the thread clipper (the arena is then in an undefined state).
-__device__ int wclip_pair(Arena &A, int op, const PolyView &subj, const PolyView &clip, WAet &W, int *mode) {
+// Horizontal state before each lane's slot and after the chunk (hstate_*):
+// one-sided edges (exists 1 or 2) move NH to BH/TH and BH/TH back to NH;
+// two-sided edges (exists 3) swap BH and TH; `x` is the state a one-sided
+// edge gives when it leaves NH.
+__device__ inline int hstate_before(int carry, unsigned m1, unsigned m2, int x) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = lanemask_lt();
+  const unsigned l1 = m1 & lt;
+  const int j = l1 ? 31 - __clz(l1) : lane;
+  const int xj = __shfl_sync(kFull, x, j);
+  const bool nonNH = (carry != NH) ^ (__popc(l1) & 1);
+  if (!nonNH) return NH;
+  const int from = l1 ? xj : carry;
+  const unsigned between = l1 ? (m2 & lt & ~((2u << j) - 1u)) : (m2 & lt);
+  return (__popc(between) & 1) ? 3 - from : from;
+}
+
+__device__ inline int hstate_after(int carry, unsigned m1, unsigned m2, int x) {
+  const int last = m1 ? 31 - __clz(m1) : -1;
+  const int xl = __shfl_sync(kFull, x, last < 0 ? 0 : last);
+  const bool nonNH = (carry != NH) ^ (__popc(m1) & 1);
+  if (!nonNH) return NH;
+  const int from = last >= 0 ? xl : carry;
+  const unsigned between = last >= 0 ? (m2 & ~((2u << last) - 1u)) : m2;
+  return (__popc(between) & 1) ? 3 - from : from;
+}
+
+template <int op>
+__device__ __noinline__ int wclip_impl(Arena &A, const PolyView &subj, const PolyView &clip, WAet &W, int *mode) {
   const int lane = threadIdx.x & 31;
   *mode = kWarpOk;
   const int sn = (int)(subj.r1 - subj.r0), cn = (int)(clip.r1 - clip.r0);
   if ((sn == 0 && cn == 0) || (sn == 0 && (op == OP_INT || op == OP_DIFF)) || (cn == 0 && op == OP_INT)) return -1;
-  int nsbt = 0;
-  if (!wbuild(A, op, subj, clip, W, &nsbt)) {
+  if (!wbuild(A, op, subj, clip, W)) {
     *mode = kWarpFallback;
     return -1;
   }
   if (A.status || A.nb == 0) return -1;
 
   const int pC0 = op == OP_DIFF ? RIGHT : LEFT;
+  const WPoly P{wsm_polys(W.scap), A.P, W.spcap};
   int n = 0;  // active edges (slots)
-  int out_poly = -1, lmin = 0, scanbeam = 0;
+  int out_poly = -1, lmin = 0;
   int cf = -1;  // current output fragment; lane 0 only, carried across beams as in GPC
-  double yb, yt = 0.0, dy = 0.0;
-  while (scanbeam < nsbt) {
-    yb = A.Y[scanbeam++].y;
-    if (scanbeam < nsbt) {
-      yt = A.Y[scanbeam].y;
-      dy = yt - yb;
+  double yt = 0.0, dy = 0.0;
+  // the next 32 local-minimum ys, one per lane
+  int bbase = 0;
+  double bwin = lane < A.nb ? A.B[lane].y : 0.0;
+  auto bys = [&](int i) -> double {
+    if (i - bbase >= 32) {
+      bbase += 32 * ((i - bbase) / 32);
+      bwin = bbase + lane < A.nb ? A.B[bbase + lane].y : 0.0;
     }
+    return __shfl_sync(kFull, bwin, i - bbase);
+  };
+  double yb = bys(0);  // the lowest vertex is a local minimum
+  for (;;) {
     // ---- local minima at yb into the AET (add_edge_to_aet)
-    while (lmin < A.nb && A.B[lmin].y == yb) {
+    while (lmin < A.nb && bys(lmin) == yb) {
       const int e = A.B[lmin++].edge;
       if (n >= W.cap) {
-        *mode = kWarpFallback;
-        return -1;
+        // the table outgrows its slots: move it to the arena's overflow area,
+        // sized for every edge of the pair
+        const int big = (A.cap.e + 31) / 32 * 32;
+        if (n >= big || W.base != prt_wsm) {
+          *mode = kWarpFallback;
+          return -1;
+        }
+        WAet G = W;
+        G.base = reinterpret_cast<unsigned char *>(A.E) + arena_bytes(A.cap);
+        G.cap = big;
+        for (int k = lane; k < n; k += 32) wstore(G, k, wload(W, k));
+        __syncwarp();
+        W = G;
       }
       const WSlot ns = wslot_of(A, e);
       int pos = n;
@@ -500,8 +639,8 @@ __device__ int wclip_pair(Arena &A, int op, const PolyView &subj, const PolyView
         const int s = c + lane;
         bool hit = false;
         if (s < n) {
-          const double sxb = W.xb[s];
-          hit = ns.xb < sxb || (ns.xb == sxb && ns.dx < W.dx[s]);
+          const double sxb = W.xb()[s];
+          hit = ns.xb < sxb || (ns.xb == sxb && ns.dx < W.dx()[s]);
         }
         const unsigned m = __ballot_sync(kFull, hit);
         if (m) {
@@ -521,12 +660,16 @@ __device__ int wclip_pair(Arena &A, int op, const PolyView &subj, const PolyView
       __syncwarp();
       n++;
     }
-    if (n == 0) continue;
+    if (n == 0) {
+      if (lmin >= A.nb) break;
+      yb = bys(lmin);
+      continue;
+    }
 
     // ---- bundles above yb (GPC:371-393)
     {
-      int cj = -1;       // last slot so far whose edge does not end at yb
-      int cacc = 0;      // its accumulated bundle bits
+      int cj = -1;   // last slot so far whose edge does not end at yb
+      int cacc = 0;  // its accumulated bundle bits
       double cxb = 0.0, cdx = 0.0;
       for (int c = 0; c < n; c += 32) {
         const int s = c + lane;
@@ -534,10 +677,10 @@ __device__ int wclip_pair(Arena &A, int op, const PolyView &subj, const PolyView
         double xb = 0.0, dx = 0.0, ty = 0.0;
         uint32_t fl = 0;
         if (valid) {
-          xb = W.xb[s];
-          dx = W.dx[s];
-          ty = W.ty[s];
-          fl = W.fl[s];
+          xb = W.xb()[s];
+          dx = W.dx()[s];
+          ty = W.ty()[s];
+          fl = W.fl()[s];
         }
         const bool f = valid && ty != yb;
         const unsigned mf = __ballot_sync(kFull, f);
@@ -559,17 +702,19 @@ __device__ int wclip_pair(Arena &A, int op, const PolyView &subj, const PolyView
         const unsigned ml = __ballot_sync(kFull, link);
         // accumulated bits: XOR of onehot(type) along linked chains
         int acc = f ? (1 << (fl & W_TYPE)) : 0;
-        int ptr = link ? (lower ? pj : 32) : -1;  // 32 = the carried slot of earlier chunks
-        for (int d = 0; d < 5; d++) {
-          const int src = (ptr >= 0 && ptr < 32) ? ptr : lane;
-          const int a2 = __shfl_sync(kFull, acc, src);
-          const int p2 = __shfl_sync(kFull, ptr, src);
-          if (ptr >= 0 && ptr < 32) {
-            acc ^= a2;
-            ptr = p2;
+        if (ml) {
+          int ptr = link ? (lower ? pj : 32) : -1;  // 32 = the carried slot of earlier chunks
+          for (int d = 0; d < 5; d++) {
+            const int src = (ptr >= 0 && ptr < 32) ? ptr : lane;
+            const int a2 = __shfl_sync(kFull, acc, src);
+            const int p2 = __shfl_sync(kFull, ptr, src);
+            if (ptr >= 0 && ptr < 32) {
+              acc ^= a2;
+              ptr = p2;
+            }
           }
+          if (ptr == 32) acc ^= cacc;
         }
-        if (ptr == 32) acc ^= cacc;
         // a linked successor within the chunk makes this slot a tail
         const unsigned upper = mf & ~lanemask_lt() & ~(1u << lane);
         const int nj = upper ? __ffs(upper) - 1 : -1;
@@ -586,12 +731,12 @@ __device__ int wclip_pair(Arena &A, int op, const PolyView &subj, const PolyView
             ba = acc;
             st = UNBUNDLED;
           }
-          W.fl[s] = fset(fset(fl, W_BA, ba), W_STA, st);
+          W.fl()[s] = fset(fset(fl, W_BA, ba), W_STA, st);
         }
         // the first linked slot of this chunk makes the carried slot a tail
         if (mf && cj >= 0) {
           const int first = __ffs(mf) - 1;
-          if (((ml >> first) & 1u) && lane == 0) W.fl[cj] = fset(fset(W.fl[cj], W_BA, 0), W_STA, BUNDLE_TAIL);
+          if (((ml >> first) & 1u) && lane == 0) W.fl()[cj] = fset(fset(W.fl()[cj], W_BA, 0), W_STA, BUNDLE_TAIL);
         }
         if (mf) {
           const int lj = 31 - __clz(mf);
@@ -605,202 +750,178 @@ __device__ int wclip_pair(Arena &A, int op, const PolyView &subj, const PolyView
     }
 
     // ---- parity, horizontal state, vertex classes (GPC:395-423)
-    unsigned any_contrib = 0;
+    // Parity before a slot is the XOR of the above-bundle bits before it (a
+    // popcount of a ballot); the horizontal state follows from the last
+    // one-sided edge before it and the two-sided edges in between.
+    bool any_contrib = false, any_fix = false;
     {
       int parC = pC0, parS = LEFT;
       int hC = NH, hS = NH;
+      double cpx = -kDblMax;  // GPC's px carried across chunks
       for (int c = 0; c < n; c += 32) {
         const int s = c + lane;
         const bool valid = s < n;
-        uint32_t fl = valid ? W.fl[s] : 0u;
+        uint32_t fl = valid ? W.fl()[s] : 0u;
         const int ba = fbits(fl, W_BA), bb = fbits(fl, W_BB);
         const int aC = ba & 1, aS = ba >> 1, bC = bb & 1, bS = bb >> 1;
         const int exC = aC + (bC << 1), exS = aS + (bS << 1);
-        // exclusive XOR scans of the parities
-        int xC = aC, xS = aS;
-        for (int d = 1; d < 32; d <<= 1) {
-          const int tC = __shfl_up_sync(kFull, xC, d), tS = __shfl_up_sync(kFull, xS, d);
-          if (lane >= d) {
-            xC ^= tC;
-            xS ^= tS;
-          }
-        }
-        const int pCb = parC ^ xC ^ aC, pSb = parS ^ xS ^ aS;  // before this slot
-        const int pCa = pCb ^ aC, pSa = pSb ^ aS;              // after it
-        // horizontal-state transitions, composed by an inclusive scan
-        uint32_t fC = kHfIdentity, fS = kHfIdentity;
-        if (exC) {
-          const int col = ((exC - 1) << 1) + pCa;
-          fC = (uint32_t)c_wnext_h[0][col] | ((uint32_t)c_wnext_h[1][col] << 2) | ((uint32_t)c_wnext_h[2][col] << 4);
-        }
-        if (exS) {
-          const int col = ((exS - 1) << 1) + pSa;
-          fS = (uint32_t)c_wnext_h[0][col] | ((uint32_t)c_wnext_h[1][col] << 2) | ((uint32_t)c_wnext_h[2][col] << 4);
-        }
-        for (int d = 1; d < 32; d <<= 1) {
-          const uint32_t tC = __shfl_up_sync(kFull, fC, d), tS = __shfl_up_sync(kFull, fS, d);
-          if (lane >= d) {
-            fC = hf_compose(fC, tC);
-            fS = hf_compose(fS, tS);
-          }
-        }
-        uint32_t eC = __shfl_up_sync(kFull, fC, 1), eS = __shfl_up_sync(kFull, fS, 1);
-        if (lane == 0) {
-          eC = kHfIdentity;
-          eS = kHfIdentity;
-        }
-        const int horC = (int)hf_apply(eC, hC), horS = (int)hf_apply(eS, hS);
+        const unsigned lt = lanemask_lt();
+        const unsigned maC = __ballot_sync(kFull, aC), maS = __ballot_sync(kFull, aS);
+        const int pCb = parC ^ (__popc(maC & lt) & 1), pSb = parS ^ (__popc(maS & lt) & 1);
+        const int pCa = pCb ^ aC, pSa = pSb ^ aS;
+        const unsigned m1C = __ballot_sync(kFull, exC == 1 || exC == 2), m2C = __ballot_sync(kFull, exC == 3);
+        const unsigned m1S = __ballot_sync(kFull, exS == 1 || exS == 2), m2S = __ballot_sync(kFull, exS == 3);
+        const int xC = ((exC == 2) ^ pCa) ? TH : BH, xS = ((exS == 2) ^ pSa) ? TH : BH;
+        const int horC = hstate_before(hC, m1C, m2C, xC), horS = hstate_before(hS, m1S, m2S, xS);
         const bool exists = valid && (exC || exS);
         bool contributing = false;
+        int vclass = 0;
         if (exists) {
           const int hc = horC != NH, hs = horS != NH;
           int br = 0, bl = 0, tr = 0, tl = 0;
-          switch (op) {
-            case OP_DIFF:
-            case OP_INT:
-              contributing = (exC && (pSb || horS)) || (exS && (pCb || horC)) || (exC && exS && (pCb == pSb));
-              br = pCb && pSb;
-              bl = (pCb ^ aC) && (pSb ^ aS);
-              tr = (pCb ^ hc) && (pSb ^ hs);
-              tl = (pCb ^ hc ^ bC) && (pSb ^ hs ^ bS);
-              break;
-            case OP_XOR:
-              contributing = exC || exS;
-              br = pCb ^ pSb;
-              bl = (pCb ^ aC) ^ (pSb ^ aS);
-              tr = (pCb ^ hc) ^ (pSb ^ hs);
-              tl = (pCb ^ hc ^ bC) ^ (pSb ^ hs ^ bS);
-              break;
-            default:
-              contributing = (exC && (!pSb || horS)) || (exS && (!pCb || horC)) || (exC && exS && (pCb == pSb));
-              br = pCb || pSb;
-              bl = (pCb ^ aC) || (pSb ^ aS);
-              tr = (pCb ^ hc) || (pSb ^ hs);
-              tl = (pCb ^ hc ^ bC) || (pSb ^ hs ^ bS);
-              break;
+          if (op == OP_DIFF || op == OP_INT) {
+            contributing = (exC && (pSb || horS)) || (exS && (pCb || horC)) || (exC && exS && (pCb == pSb));
+            br = pCb && pSb;
+            bl = (pCb ^ aC) && (pSb ^ aS);
+            tr = (pCb ^ hc) && (pSb ^ hs);
+            tl = (pCb ^ hc ^ bC) && (pSb ^ hs ^ bS);
+          } else if (op == OP_XOR) {
+            contributing = exC || exS;
+            br = pCb ^ pSb;
+            bl = (pCb ^ aC) ^ (pSb ^ aS);
+            tr = (pCb ^ hc) ^ (pSb ^ hs);
+            tl = (pCb ^ hc ^ bC) ^ (pSb ^ hs ^ bS);
+          } else {
+            contributing = (exC && (!pSb || horS)) || (exS && (!pCb || horC)) || (exC && exS && (pCb == pSb));
+            br = pCb || pSb;
+            bl = (pCb ^ aC) || (pSb ^ aS);
+            tr = (pCb ^ hc) || (pSb ^ hs);
+            tl = (pCb ^ hc ^ bC) || (pSb ^ hs ^ bS);
           }
-          const int vclass = tr + (tl << 1) + (br << 2) + (bl << 3);
+          vclass = tr + (tl << 1) + (br << 2) + (bl << 3);
           fl = fset(fl, W_SIDE, pCb | (pSb << 1));
-          fl = (fl & ~(15u << W_VC) & ~W_CONTRIB & ~W_STARTS) | ((uint32_t)vclass << W_VC);
-          if (contributing) {
-            fl |= W_CONTRIB;
-            if ((vclass == LED || vclass == RED) && A.E[W.edge[s]].by == yb) fl |= W_STARTS;
-          }
-          W.fl[s] = fl;
-        } else if (valid) {
-          W.fl[s] = fl & ~W_CONTRIB;
+          fl = (fl & ~(15u << W_VC) & ~W_STARTS & ~W_PXNE) | ((uint32_t)vclass << W_VC);
+          if (contributing && (vclass == LED || vclass == RED) && W.by()[s] == yb) fl |= W_STARTS;
         }
-        any_contrib |= __ballot_sync(kFull, contributing);
-        const int lastC = __shfl_sync(kFull, pCa, 31), lastS = __shfl_sync(kFull, pSa, 31);
-        const uint32_t gC = __shfl_sync(kFull, fC, 31), gS = __shfl_sync(kFull, fS, 31);
-        parC = lastC;
-        parS = lastS;
-        hC = (int)hf_apply(gC, hC);
-        hS = (int)hf_apply(gS, hS);
+        // GPC's px before a slot: the xb of the last contributing slot before
+        // it whose class the output step handles (each of those leaves px = xb)
+        const bool handled = contributing && vclass != NUL && vclass != TED && vclass != BED && vclass != FUL;
+        const unsigned mh = __ballot_sync(kFull, handled);
+        const unsigned lh = mh & lt;
+        const double xbs = valid ? W.xb()[s] : 0.0;
+        const double pxl = __shfl_sync(kFull, xbs, lh ? 31 - __clz(lh) : lane);
+        const double px_before = lh ? pxl : cpx;
+        if (mh) cpx = __shfl_sync(kFull, xbs, 31 - __clz(mh));
+        // continuing left / right edges only pass their output polygon up:
+        // done here; the rest are events for the serial step
+        const bool copy = contributing && (vclass == LED || vclass == RED) && !(fl & W_STARTS);
+        if (exists) {
+          if (xbs != px_before) fl |= W_PXNE;
+          W.fl()[s] = fl;
+          if (copy) W.outA()[s] = W.outB()[s];
+        }
+        const unsigned mc = __ballot_sync(kFull, contributing && !copy);
+        if (lane == 0) W.cmask()[c >> 5] = mc;
+        any_contrib |= mc != 0;
+        any_fix |= __any_sync(kFull, valid && W.ty()[s] == yb && fbits(fl, W_STB) == BUNDLE_HEAD);
+        parC ^= __popc(maC) & 1;
+        parS ^= __popc(maS) & 1;
+        hC = hstate_after(hC, m1C, m2C, xC);
+        hS = hstate_after(hS, m1S, m2S, xS);
         __syncwarp();
       }
     }
 
-    // ---- output, in AET order (lane 0; GPC:425-570)
+    // ---- output, in AET order (GPC:425-570): lane 0 runs GPC's serial
+    // bookkeeping for the event slots; a contour merge's redirect runs on the
+    // whole warp
     if (any_contrib) {
-      if (lane == 0) {
-        double px = -kDblMax;
-        for (int s = 0; s < n && !A.status; s++) {
-          const uint32_t fl = W.fl[s];
-          if (!(fl & W_CONTRIB)) continue;
-          const int vclass = (int)((fl >> W_VC) & 15u);
-          const double xb = W.xb[s];
-          int &oa = W.outA[s];
-          int &ob = W.outB[s];
-          switch (vclass) {
-            case EMN:
-            case IMN: {
-              const int k = w_add_local_min(A, out_poly, xb, yb);
-              if (k >= 0) oa = k;
-              px = xb;
-              cf = oa;
-              break;
+      for (int c = 0; c < n; c += 32) {
+        unsigned m = W.cmask()[c >> 5];
+        while (m) {
+          const int s = c + __ffs(m) - 1;
+          m &= m - 1;
+          int rt = -1, rto = -1;
+          if (lane == 0 && !A.status) {
+            const uint32_t fl = W.fl()[s];
+            const int vclass = (int)((fl >> W_VC) & 15u);
+            const double xb = W.xb()[s];
+            const bool pxne = (fl & W_PXNE) != 0;
+            int &oa = W.outA()[s];
+            int &ob = W.outB()[s];
+            switch (vclass) {
+              case EMN:
+              case IMN: {
+                const int k = wp_local_min(A, P, out_poly, xb, yb);
+                if (k >= 0) oa = k;
+                cf = oa;
+                break;
+              }
+              case ERI:
+                if (pxne) wp_add_right(A, P, cf, xb, yb);
+                oa = cf;
+                cf = -1;
+                break;
+              case ELI:
+                wp_add_left(A, P, ob, xb, yb);
+                cf = ob;
+                break;
+              case EMX:
+                if (pxne) wp_add_left(A, P, cf, xb, yb);
+                rt = wp_merge_right(A, P, cf, ob, &rto);
+                cf = -1;
+                break;
+              case ILI:
+                if (pxne) wp_add_left(A, P, cf, xb, yb);
+                oa = cf;
+                cf = -1;
+                break;
+              case IRI:
+                wp_add_right(A, P, ob, xb, yb);
+                cf = ob;
+                ob = -1;
+                break;
+              case IMX:
+                if (pxne) wp_add_right(A, P, cf, xb, yb);
+                rt = wp_merge_left(A, P, cf, ob, &rto);
+                cf = -1;
+                ob = -1;
+                break;
+              case IMM: {
+                if (pxne) wp_add_right(A, P, cf, xb, yb);
+                rt = wp_merge_left(A, P, cf, ob, &rto);
+                ob = -1;
+                const int k = wp_local_min(A, P, out_poly, xb, yb);
+                if (k >= 0) oa = k;
+                cf = oa;
+                break;
+              }
+              case EMM: {
+                if (pxne) wp_add_left(A, P, cf, xb, yb);
+                rt = wp_merge_right(A, P, cf, ob, &rto);
+                ob = -1;
+                const int k = wp_local_min(A, P, out_poly, xb, yb);
+                if (k >= 0) oa = k;
+                cf = oa;
+                break;
+              }
+              case LED:
+                if (fl & W_STARTS) wp_add_left(A, P, ob, xb, yb);
+                oa = ob;
+                break;
+              case RED:
+                if (fl & W_STARTS) wp_add_right(A, P, ob, xb, yb);
+                oa = ob;
+                break;
+              default:
+                break;
             }
-            case ERI:
-              if (xb != px) {
-                add_right(A, cf, xb, yb);
-                px = xb;
-              }
-              oa = cf;
-              cf = -1;
-              break;
-            case ELI:
-              add_left(A, ob, xb, yb);
-              px = xb;
-              cf = ob;
-              break;
-            case EMX:
-              if (xb != px) {
-                add_left(A, cf, xb, yb);
-                px = xb;
-              }
-              merge_right(A, cf, ob, out_poly);
-              cf = -1;
-              break;
-            case ILI:
-              if (xb != px) {
-                add_left(A, cf, xb, yb);
-                px = xb;
-              }
-              oa = cf;
-              cf = -1;
-              break;
-            case IRI:
-              add_right(A, ob, xb, yb);
-              px = xb;
-              cf = ob;
-              ob = -1;
-              break;
-            case IMX:
-              if (xb != px) {
-                add_right(A, cf, xb, yb);
-                px = xb;
-              }
-              merge_left(A, cf, ob, out_poly);
-              cf = -1;
-              ob = -1;
-              break;
-            case IMM: {
-              if (xb != px) {
-                add_right(A, cf, xb, yb);
-                px = xb;
-              }
-              merge_left(A, cf, ob, out_poly);
-              ob = -1;
-              const int k = w_add_local_min(A, out_poly, xb, yb);
-              if (k >= 0) oa = k;
-              cf = oa;
-              break;
-            }
-            case EMM: {
-              if (xb != px) {
-                add_left(A, cf, xb, yb);
-                px = xb;
-              }
-              merge_right(A, cf, ob, out_poly);
-              ob = -1;
-              const int k = w_add_local_min(A, out_poly, xb, yb);
-              if (k >= 0) oa = k;
-              cf = oa;
-              break;
-            }
-            case LED:
-              if (fl & W_STARTS) add_left(A, ob, xb, yb);
-              oa = ob;
-              px = xb;
-              break;
-            case RED:
-              if (fl & W_STARTS) add_right(A, ob, xb, yb);
-              oa = ob;
-              px = xb;
-              break;
-            default:
-              break;
+          }
+          rt = __shfl_sync(kFull, rt, 0);
+          if (rt >= 0) {
+            // the new local minimum of IMM / EMM (if any) is past the old list
+            // and never has proxy rt, so the pass may include it
+            wp_redirect_all(P, __shfl_sync(kFull, A.np, 0), rt, __shfl_sync(kFull, rto, 0));
           }
         }
       }
@@ -810,55 +931,76 @@ __device__ int wclip_pair(Arena &A, int op, const PolyView &subj, const PolyView
       if (A.status) return -1;
     }
 
-    // ---- delete edges ending at yb, compute xt (GPC:426-459)
+    // ---- next scanbeam, delete edges ending at yb, compute xt (GPC:426-459)
+    bool last;
     {
-      // bundle fix-ups of deleted bundle heads, in AET order (lane 0)
-      bool fix = false;
-      for (int c = 0; c < n; c += 32) {
-        const int s = c + lane;
-        fix |= s < n && W.ty[s] == yb && fbits(W.fl[s], W_STB) == BUNDLE_HEAD;
-      }
-      if (__any_sync(kFull, fix)) {
+      if (any_fix) {
+        // bundle fix-ups of deleted bundle heads, in AET order (lane 0)
         if (lane == 0) {
           for (int d = 0; d < n; d++) {
-            if (!(W.ty[d] == yb && fbits(W.fl[d], W_STB) == BUNDLE_HEAD)) continue;
+            if (!(W.ty()[d] == yb && fbits(W.fl()[d], W_STB) == BUNDLE_HEAD)) continue;
             int pe = d - 1;
-            while (pe >= 0 && W.ty[pe] == yb) pe--;
+            while (pe >= 0 && W.ty()[pe] == yb) pe--;
             if (pe < 0) continue;
-            if (fbits(W.fl[pe], W_STB) == BUNDLE_TAIL) {
-              W.outB[pe] = W.outB[d];
-              W.fl[pe] = fset(W.fl[pe], W_STB, UNBUNDLED);
+            if (fbits(W.fl()[pe], W_STB) == BUNDLE_TAIL) {
+              W.outB()[pe] = W.outB()[d];
+              W.fl()[pe] = fset(W.fl()[pe], W_STB, UNBUNDLED);
               int pp = pe - 1;
-              while (pp >= 0 && W.ty[pp] == yb) pp--;
-              if (pp >= 0 && fbits(W.fl[pp], W_STB) == BUNDLE_TAIL) W.fl[pe] = fset(W.fl[pe], W_STB, BUNDLE_HEAD);
+              while (pp >= 0 && W.ty()[pp] == yb) pp--;
+              if (pp >= 0 && fbits(W.fl()[pp], W_STB) == BUNDLE_TAIL) W.fl()[pe] = fset(W.fl()[pe], W_STB, BUNDLE_HEAD);
             }
           }
         }
         __syncwarp();
       }
+      // the next scanbeam y: the lowest top of the edges that go on, or the
+      // next local minimum
+      double ny = lmin < A.nb ? bys(lmin) : kInf;
+      for (int c = 0; c < n; c += 32) {
+        const int s = c + lane;
+        const double ty = s < n ? W.ty()[s] : kInf;
+        double m = ty != yb ? ty : kInf;
+        for (int o = 16; o; o >>= 1) {
+          const double t = __shfl_xor_sync(kFull, m, o);
+          m = t < m ? t : m;
+        }
+        ny = m < ny ? m : ny;
+      }
+      last = !(ny < kInf);
+      if (!last) {
+        yt = ny;
+        dy = yt - yb;
+      }
       int kept = 0;
       for (int c = 0; c < n; c += 32) {
         const int s = c + lane;
-        WSlot v;
-        bool keep = false;
-        if (s < n) {
-          v = wload(W, s);
-          keep = v.ty != yb;
-          if (keep) {
-            const Edge &E = A.E[v.edge];
-            if (v.ty == yt) v.xt = E.tx;
-            else v.xt = E.bx + v.dx * (yt - E.by);
-          }
-        }
+        const bool valid = s < n;
+        const double ty = valid ? W.ty()[s] : 0.0;
+        const bool keep = valid && ty != yb;
         const unsigned m = __ballot_sync(kFull, keep);
-        __syncwarp();
-        if (keep) wstore(W, kept + __popc(m & lanemask_lt()), v);
+        const unsigned vm = __ballot_sync(kFull, valid);
+        double xt = 0.0;
+        if (keep) {
+          if (ty == yt) xt = W.tx()[s];
+          else xt = W.bx()[s] + W.dx()[s] * (yt - W.by()[s]);
+        }
+        if (kept == c && m == vm) {
+          if (keep) W.xt()[s] = xt;  // nothing deleted so far: in place
+        } else {
+          WSlot v;
+          if (keep) {
+            v = wload(W, s);
+            v.xt = xt;
+          }
+          __syncwarp();
+          if (keep) wstore(W, kept + __popc(m & lanemask_lt()), v);
+        }
         kept += __popc(m);
         __syncwarp();
       }
       n = kept;
     }
-    if (scanbeam >= nsbt) continue;
+    if (last) break;
 
     // ---- intersections (GPC:461-659)
     {
@@ -870,11 +1012,11 @@ __device__ int wclip_pair(Arena &A, int op, const PolyView &subj, const PolyView
         bool el = false;
         double xb = 0.0, xt = 0.0, dx = 0.0;
         if (s < n) {
-          const uint32_t fl = W.fl[s];
+          const uint32_t fl = W.fl()[s];
           el = fbits(fl, W_STA) == BUNDLE_HEAD || fbits(fl, W_BA) != 0;
-          xb = W.xb[s];
-          xt = W.xt[s];
-          dx = W.dx[s];
+          xb = W.xb()[s];
+          xt = W.xt()[s];
+          dx = W.dx()[s];
         }
         const unsigned me = __ballot_sync(kFull, el);
         const unsigned lower = me & lanemask_lt();
@@ -907,17 +1049,18 @@ __device__ int wclip_pair(Arena &A, int op, const PolyView &subj, const PolyView
         // spill to the linked form, run the thread clipper's step, reload
         for (int c = 0; c < n; c += 32) {
           const int s = c + lane;
-          if (s < n) wspill(A, wload(W, s), s > 0 ? W.edge[s - 1] : -1, s + 1 < n ? W.edge[s + 1] : -1);
+          if (s < n) wspill(A, wload(W, s), s > 0 ? W.edge()[s - 1] : -1, s + 1 < n ? W.edge()[s + 1] : -1);
         }
         __syncwarp();
+        wp_sync(P, A.np, 0);
         int bad = 0;
         if (lane == 0) {
-          int aet = W.edge[0];
+          int aet = W.edge()[0];
           intersect_beam(A, op, aet, out_poly, yb, dy);
           if (!A.status) {
             int cur = aet, k = 0;
             while (cur >= 0 && k < n) {
-              W.ord[k++] = cur;
+              W.ord()[k++] = cur;
               cur = A.E[cur].next;
             }
             bad = (k != n || cur >= 0) ? 1 : 0;
@@ -927,6 +1070,7 @@ __device__ int wclip_pair(Arena &A, int op, const PolyView &subj, const PolyView
         A.status = __shfl_sync(kFull, A.status, 0);
         out_poly = __shfl_sync(kFull, out_poly, 0);
         bad = __shfl_sync(kFull, bad, 0);
+        wp_sync(P, A.np, 1);
         if (bad) {
           *mode = kWarpFallback;
           return -1;
@@ -935,7 +1079,7 @@ __device__ int wclip_pair(Arena &A, int op, const PolyView &subj, const PolyView
         for (int c = 0; c < n; c += 32) {
           const int s = c + lane;
           WSlot v;
-          if (s < n) v = wslot_of(A, W.ord[s]);
+          if (s < n) v = wslot_of(A, W.ord()[s]);
           __syncwarp();
           if (s < n) wstore(W, s, v);
         }
@@ -947,23 +1091,42 @@ __device__ int wclip_pair(Arena &A, int op, const PolyView &subj, const PolyView
     for (int c = 0; c < n; c += 32) {
       const int s = c + lane;
       if (s < n) {
-        WSlot v = wload(W, s);
-        const int oa = v.outA, sta = fbits(v.fl, W_STA), ba = fbits(v.fl, W_BA);
-        const int sc = v.ty == yt ? A.E[v.edge].succ : -1;
+        const uint32_t fl = W.fl()[s];
+        const int oa = W.outA()[s], sta = fbits(fl, W_STA), ba = fbits(fl, W_BA);
+        const int sc = W.ty()[s] == yt ? W.succ()[s] : -1;
         if (sc >= 0) {
-          v = wslot_of(A, sc);
+          WSlot v = wslot_of(A, sc);
+          v.outB = oa;
+          v.fl = fset(fset(v.fl, W_STB, sta), W_BB, ba);
+          v.outA = -1;
+          wstore(W, s, v);
         } else {
-          v.xb = v.xt;
+          W.outB()[s] = oa;
+          W.fl()[s] = fset(fset(fl, W_STB, sta), W_BB, ba);
+          W.xb()[s] = W.xt()[s];
+          W.outA()[s] = -1;
         }
-        v.outB = oa;
-        v.fl = fset(fset(v.fl, W_STB, sta), W_BB, ba);
-        v.outA = -1;
-        wstore(W, s, v);
       }
     }
     __syncwarp();
+    yb = yt;
   }
+  wp_sync(P, A.np, 0);  // the result readers use the arena's nodes
   return out_poly;
+}
+
+// Clips subj against clip with the calling warp (all 32 lanes, converged).
+// Returns the output polygon list head on every lane; A.status is valid on
+// every lane, the output counters (np, nvx) on lane 0.  *mode =
+// kWarpFallback when the pair needs the thread clipper (the arena is then in
+// an undefined state).
+__device__ inline int wclip_pair(Arena &A, int op, const PolyView &subj, const PolyView &clip, WAet &W, int *mode) {
+  switch (op) {
+    case OP_DIFF: return wclip_impl<OP_DIFF>(A, subj, clip, W, mode);
+    case OP_INT: return wclip_impl<OP_INT>(A, subj, clip, W, mode);
+    case OP_XOR: return wclip_impl<OP_XOR>(A, subj, clip, W, mode);
+    default: return wclip_impl<OP_UNION>(A, subj, clip, W, mode);
+  }
 }
 
 }  // namespace gpc

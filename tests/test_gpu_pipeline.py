@@ -106,3 +106,29 @@ def test_pipeline_rejects_default_stream(cuda):
     with torch.cuda.stream(torch.cuda.default_stream()):
         with pytest.raises(prt.PrtError):
             pipe.run()
+
+
+def test_autotune_installs_a_valid_schedule(cuda, tmp_path):
+    """prt_autotune times fanouts and schedules on a sample, installs the
+    best schedule (which then gives the same contours), and its JSON cache
+    returns the same choice without timing."""
+    import parlllelrtree_b200 as prt
+
+    A, B = _layers(n=600, seed=11, zipf=1.2, nv_hi=400)
+    LA, LB = prt.Layer.from_dict(A), prt.Layer.from_dict(B)
+    saved = prt.get_schedule()
+    try:
+        cache = str(tmp_path / "tune.json")
+        r = prt.autotune(LA, LB, max_sample_pairs=2000, time_budget_s=20.0, cache=cache)
+        assert not r["cached"] and r["fanout"] in (8, 12, 16, 24, 32) and r["candidates"] >= 6
+        assert prt.get_schedule() == r["schedule"]
+        r2 = prt.autotune(LA, LB, cache=cache)
+        assert r2["cached"] and r2["schedule"] == r["schedule"]
+        t = prt.build_bottomup(LA.mbr(), fanout=r["fanout"])
+        pairs = t.join(LB.mbr(), sorted=True)
+        l2p = t.leaf_order()
+        tuned = prt.overlay(pairs, LA, LB, leaf_to_poly=l2p, sched="batched").contours()
+        plain = prt.overlay(pairs, LA, LB, leaf_to_poly=l2p, sched="plain").contours()
+        assert all(same_contours(x, y) for x, y in zip(tuned, plain))
+    finally:
+        prt.set_schedule(saved)
