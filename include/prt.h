@@ -253,16 +253,19 @@ int prt_clip_pair_host(int op, int s_ncont, const int32_t *s_nverts, const doubl
  * (bin_thresholds[b+1], bin_thresholds[b]]; bins are clipped largest first
  * in one persistent launch.  bin_warp_mode[b] = 1 clips each pair of the bin
  * with a whole warp (active edge table in shared memory, aet_slots slots per
- * warp; pairs whose table outgrows it are clipped by one thread), 0 with one
- * thread per pair.  bin_warps_per_sm[b] persistent warps per SM start on bin b
- * and steal from the smaller bins once theirs is empty. */
+ * warp, a larger table moves to the pair's arena), 0 with one
+ * thread per pair.  The launch starts warps_per_sm persistent warps per SM;
+ * every warp takes the next pair (warp mode) or the next 32 pairs (thread
+ * mode) of the largest bin that still has pairs, so the largest pairs are
+ * clipped first by all warps. */
 #define PRT_MAX_BINS 8
 typedef struct {
   int32_t nbins;
   int32_t aet_slots;
   int64_t bin_thresholds[PRT_MAX_BINS];
   int32_t bin_warp_mode[PRT_MAX_BINS];
-  int32_t bin_warps_per_sm[PRT_MAX_BINS];
+  int32_t warps_per_sm;
+  int32_t reserved;
 } prt_schedule;
 
 /* Sets the schedule used by later calls of this process (NULL restores the

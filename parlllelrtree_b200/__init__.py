@@ -288,34 +288,33 @@ MAX_BINS = 8
 
 class _Schedule(C.Structure):
     _fields_ = [("nbins", C.c_int32), ("aet_slots", C.c_int32), ("bin_thresholds", C.c_int64 * MAX_BINS),
-                ("bin_warp_mode", C.c_int32 * MAX_BINS), ("bin_warps_per_sm", C.c_int32 * MAX_BINS)]
+                ("bin_warp_mode", C.c_int32 * MAX_BINS), ("warps_per_sm", C.c_int32), ("reserved", C.c_int32)]
 
     @classmethod
     def from_dict(cls, d: dict) -> "_Schedule":
         s = cls()
         thr = list(d["thresholds"])
         s.nbins = len(thr)
-        s.aet_slots = int(d.get("aet_slots", 256))
-        wm = list(d.get("warp_mode", [0] * len(thr)))
-        wps = list(d.get("warps_per_sm", [4] * len(thr)))
+        s.aet_slots = int(d.get("aet_slots", 128))
+        wm = list(d.get("warp_mode", [1] * len(thr)))
+        s.warps_per_sm = int(d.get("warps_per_sm", 8))
         for b in range(len(thr)):
             s.bin_thresholds[b] = int(thr[b])
             s.bin_warp_mode[b] = int(wm[b])
-            s.bin_warps_per_sm[b] = int(wps[b])
         return s
 
     def to_dict(self) -> dict:
         n = self.nbins
         return {"thresholds": [int(self.bin_thresholds[b]) for b in range(n)],
                 "warp_mode": [int(self.bin_warp_mode[b]) for b in range(n)],
-                "warps_per_sm": [int(self.bin_warps_per_sm[b]) for b in range(n)],
-                "aet_slots": int(self.aet_slots)}
+                "warps_per_sm": int(self.warps_per_sm), "aet_slots": int(self.aet_slots)}
 
 
 def get_schedule() -> dict:
     """The batched schedule in use (prt_schedule_get): size-bin thresholds
     (descending vertex-count upper bounds), per-bin warp mode (1 = one pair
-    per warp) and persistent warps per SM, and the warp clipper's AET slots."""
+    per warp), persistent warps per SM, and the warp clipper's shared-memory
+    slots."""
     s = _Schedule()
     check(lib().prt_schedule_get(C.byref(s)))
     return s.to_dict()

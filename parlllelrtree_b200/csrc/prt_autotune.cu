@@ -7,9 +7,9 @@
 //    differs.
 // 2. Batched schedule: coordinate descent over (a) the vertex count above
 //    which a pair is clipped by a whole warp, (b) the warp clipper's
-//    shared-memory slots per warp, (c) the persistent warps per SM of the
-//    warp and thread bins, each candidate timed on an evenly strided sample of
-//    the candidate pairs with CUDA events on the caller's stream.
+//    shared-memory slots per warp, (c) the persistent warps per SM, each
+//    candidate timed on an evenly strided sample of the candidate pairs with
+//    CUDA events on the caller's stream.
 // The best schedule is installed with prt_schedule_set and returned.
 #include <cuda_runtime.h>
 
@@ -38,7 +38,7 @@ struct Timer {
 };
 
 // Schedule with pairs above warp_above vertices in warp mode.
-prt_schedule make_schedule(int64_t warp_above, int slots, int warps_w, int warps_t) {
+prt_schedule make_schedule(int64_t warp_above, int slots, int warps) {
   std::vector<int64_t> thr = {1ll << 40, 4096, 1024, 256, 64};
   if (warp_above > 64 && warp_above < 4096) thr.push_back(warp_above);
   std::sort(thr.begin(), thr.end(), std::greater<int64_t>());
@@ -47,11 +47,11 @@ prt_schedule make_schedule(int64_t warp_above, int slots, int warps_w, int warps
   memset(&s, 0, sizeof s);
   s.nbins = (int)std::min<size_t>(thr.size(), PRT_MAX_BINS);
   s.aet_slots = slots;
+  s.warps_per_sm = warps;
   for (int b = 0; b < s.nbins; b++) {
     const int64_t lower = b + 1 < s.nbins ? thr[b + 1] : 0;  // bin b: (lower, thr[b]]
     s.bin_thresholds[b] = thr[b];
     s.bin_warp_mode[b] = lower >= warp_above ? 1 : 0;
-    s.bin_warps_per_sm[b] = s.bin_warp_mode[b] ? warps_w : warps_t;
   }
   return s;
 }
@@ -167,16 +167,16 @@ int prt_autotune(const prt_layer *base, const prt_layer *overlay, int op, int64_
     out->candidates++;
     return PRT_OK;
   };
-  int64_t warp_above = 256;
-  int slots = 128, ww = 2, wt = 1;
-  prt_schedule best = make_schedule(warp_above, slots, ww, wt);
+  int64_t warp_above = 64;
+  int slots = 128, wps = 8;
+  prt_schedule best = make_schedule(warp_above, slots, wps);
   double best_ms = 1e30;
   if (!rc && m > 0) {
     rc = time_sched(best, &best_ms);
-    const int64_t cands_w[] = {0, 64, 128, 512, 1024, 4096, 1ll << 41};
+    const int64_t cands_w[] = {0, 128, 256, 1024, 1ll << 41};
     for (int64_t wa : cands_w) {
       if (rc || secs_since(t0) > time_budget_s) break;
-      prt_schedule c = make_schedule(wa, slots, ww, wt);
+      prt_schedule c = make_schedule(wa, slots, wps);
       double ms = 0;
       rc = time_sched(c, &ms);
       if (!rc && ms < best_ms) {
@@ -188,7 +188,7 @@ int prt_autotune(const prt_layer *base, const prt_layer *overlay, int op, int64_
     const int cands_s[] = {64, 256};
     for (int sl : cands_s) {
       if (rc || secs_since(t0) > time_budget_s) break;
-      prt_schedule c = make_schedule(warp_above, sl, ww, wt);
+      prt_schedule c = make_schedule(warp_above, sl, wps);
       double ms = 0;
       rc = time_sched(c, &ms);
       if (!rc && ms < best_ms) {
@@ -197,17 +197,16 @@ int prt_autotune(const prt_layer *base, const prt_layer *overlay, int op, int64_
         slots = sl;
       }
     }
-    const int cands_wp[][2] = {{1, 1}, {2, 2}, {3, 1}, {4, 2}, {6, 2}, {8, 4}};
-    for (auto &wp : cands_wp) {
+    const int cands_wp[] = {4, 6, 12, 16};
+    for (int wp : cands_wp) {
       if (rc || secs_since(t0) > time_budget_s) break;
-      prt_schedule c = make_schedule(warp_above, slots, wp[0], wp[1]);
+      prt_schedule c = make_schedule(warp_above, slots, wp);
       double ms = 0;
       rc = time_sched(c, &ms);
       if (!rc && ms < best_ms) {
         best_ms = ms;
         best = c;
-        ww = wp[0];
-        wt = wp[1];
+        wps = wp;
       }
     }
   }

@@ -327,21 +327,20 @@ size_t arena_budget() {
 }  // namespace
 
 // ---- batched schedule ----------------------------------------------------------
-// Default: pairs above 256 vertices are clipped one per warp, smaller ones one
-// per thread; the warps per SM of all bins add up to the 8 warps an SM holds
-// at the clip kernel's register count.
+// Default: pairs above 64 vertices are clipped one per warp, smaller ones one
+// per thread; 8 warps per SM, what an SM holds at the clip kernel's register
+// count.
 static prt_schedule default_schedule() {
   prt_schedule d;
   memset(&d, 0, sizeof d);
   d.nbins = 5;
   d.aet_slots = 128;
+  d.warps_per_sm = 8;
   const int64_t thr[5] = {1ll << 40, 4096, 1024, 256, 64};
-  const int32_t wm[5] = {1, 1, 1, 0, 0};
-  const int32_t wps[5] = {2, 2, 2, 1, 1};
+  const int32_t wm[5] = {1, 1, 1, 1, 0};
   for (int b = 0; b < 5; b++) {
     d.bin_thresholds[b] = thr[b];
     d.bin_warp_mode[b] = wm[b];
-    d.bin_warps_per_sm[b] = wps[b];
   }
   return d;
 }
@@ -362,12 +361,12 @@ int schedule_valid(const prt_schedule &s) {
     PRT_CHECK(s.bin_thresholds[b] > 0, PRT_ERR_INVALID, "schedule: threshold %d", b);
     PRT_CHECK(b == 0 || s.bin_thresholds[b] < s.bin_thresholds[b - 1], PRT_ERR_INVALID,
               "schedule: thresholds must descend");
-    PRT_CHECK(s.bin_warps_per_sm[b] >= 1 && s.bin_warps_per_sm[b] <= 64, PRT_ERR_INVALID,
-              "schedule: warps per SM of bin %d", b);
     PRT_CHECK(s.bin_warp_mode[b] == 0 || s.bin_warp_mode[b] == 1, PRT_ERR_INVALID, "schedule: warp mode of bin %d",
               b);
   }
   PRT_CHECK(s.bin_thresholds[0] >= (1ll << 31), PRT_ERR_INVALID, "schedule: bin 0 must hold every pair size");
+  PRT_CHECK(s.warps_per_sm >= 1 && s.warps_per_sm <= 64, PRT_ERR_INVALID, "schedule: warps_per_sm %d",
+            s.warps_per_sm);
   return PRT_OK;
 }
 
@@ -385,25 +384,21 @@ size_t plan_bins(const prt_schedule &sc, const int64_t *counts, const int64_t *m
     need[b] = counts[b] > 0 ? (sc.bin_warp_mode[b] ? sl : 32 * sl) : 0;
     any_warp |= sc.bin_warp_mode[b] && counts[b] > 0;
   }
-  size_t bytes = 0;
-  int64_t warps = 0;
-  for (int g = 0; g < sc.nbins; g++) {
-    int64_t region = 512;
-    for (int b = g; b < sc.nbins; b++) region = std::max(region, need[b]);
-    region = (region + 511) & ~(int64_t)511;
-    int64_t wg = 0;
-    if (counts[g] > 0) {
-      const int64_t per = sc.bin_warp_mode[g] ? 1 : 32;
-      wg = std::min<int64_t>((counts[g] + per - 1) / per, (int64_t)kSMs * sc.bin_warps_per_sm[g]);
-      const int64_t mem_cap = (int64_t)((budget - std::min(budget, bytes)) / (size_t)region);
-      wg = std::max<int64_t>(1, std::min(wg, mem_cap));
-    }
-    plan.warp0[g] = warps;
-    plan.arena_off[g] = (int64_t)bytes;
-    plan.region[g] = region;
-    bytes += (size_t)wg * (size_t)region;
-    warps += wg;
+  // one group: every warp starts on the largest bin and moves down as bins
+  // drain, so its arena region holds the largest need of any bin
+  int64_t region = 512, work = 0;
+  for (int b = 0; b < sc.nbins; b++) {
+    region = std::max(region, need[b]);
+    work += sc.bin_warp_mode[b] ? counts[b] : (counts[b] + 31) / 32;
   }
+  region = (region + 511) & ~(int64_t)511;
+  int64_t warps = std::min<int64_t>(work, (int64_t)kSMs * sc.warps_per_sm);
+  warps = std::min<int64_t>(warps, (int64_t)(budget / (size_t)region));
+  if (work > 0) warps = std::max<int64_t>(warps, 1);
+  for (int b = 0; b <= sc.nbins; b++) plan.warp0[b] = b == 0 ? 0 : warps;
+  plan.arena_off[0] = 0;
+  plan.region[0] = region;
+  const size_t bytes = (size_t)warps * (size_t)region;
   plan.warp0[sc.nbins] = warps;
   *smem = any_warp ? gpc::waet_bytes(sc.aet_slots) : 0;
   return bytes;

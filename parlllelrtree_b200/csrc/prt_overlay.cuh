@@ -47,9 +47,11 @@ int overlay_impl(const PairSrc &S, int64_t n, int sched, double *d_area, cudaStr
 namespace prt {
 
 // Bins of the batched schedule, size-descending: bin b holds sorted positions
-// [begin[b], end[b]); warps [warp0[g], warp0[g+1]) start on bin g, each with
-// region[g] bytes of arena (enough for one pair of bin g or any later bin in
-// warp mode, or 32 pairs in thread mode), then steal from the later bins.
+// [begin[b], end[b]).  Warps [warp0[g], warp0[g+1]) start on bin g with
+// region[g] bytes of arena each (one pair of any later bin in warp mode, or
+// 32 pairs in thread mode) and move to the later bins as bins drain; the
+// planner puts every warp in group 0, so all warps take the largest pairs
+// first.
 struct BinPlan {
   int64_t begin[PRT_MAX_BINS], end[PRT_MAX_BINS];
   int64_t warp0[PRT_MAX_BINS + 1];

@@ -1,8 +1,8 @@
 """The warp-cooperative clipper (one pair per warp, active edge table in
 shared memory) against the oracle and the reference's golden fixtures: the
-batched schedule forced to warp mode for every pair, with the default slot
-count and with 32 slots (pairs whose active edge table outgrows 32 slots are
-finished by the thread clipper)."""
+batched schedule forced to warp mode for every pair, with 256 slots and with
+32 slots (pairs whose active edge table outgrows 32 slots move it to their
+arena), and a mixed warp / thread schedule."""
 import os
 
 import numpy as np
@@ -17,9 +17,9 @@ from parlllelrtree_b200 import datagen as dg
 pytestmark = pytest.mark.gpu
 
 OPS = ["diff", "int", "xor", "union"]
-WARP = {"thresholds": [1 << 40], "warp_mode": [1], "warps_per_sm": [8], "aet_slots": 256}
-WARP32 = {"thresholds": [1 << 40], "warp_mode": [1], "warps_per_sm": [8], "aet_slots": 32}
-MIXED = {"thresholds": [1 << 40, 512, 64], "warp_mode": [1, 0, 1], "warps_per_sm": [2, 3, 4], "aet_slots": 64}
+WARP = {"thresholds": [1 << 40], "warp_mode": [1], "warps_per_sm": 8, "aet_slots": 256}
+WARP32 = {"thresholds": [1 << 40], "warp_mode": [1], "warps_per_sm": 8, "aet_slots": 32}
+MIXED = {"thresholds": [1 << 40, 512, 64], "warp_mode": [1, 0, 1], "warps_per_sm": 4, "aet_slots": 64}
 SCHEDS = {"warp": WARP, "warp32": WARP32, "mixed": MIXED}
 
 
