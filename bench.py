@@ -410,6 +410,12 @@ def secondary(prt, boxes, flush, world):
     res["join_1M_windows_pairs_s"] = npairs / (ms * 1e-3)
     res["join_1M_windows_pairs"] = npairs
 
+    # the batched uneven overlay at a tenth of its size (1M x 1M takes ~10 min
+    # with the plain schedule; its numbers are in the design notes)
+    res["uneven_overlay_0.1"] = batched_overlay(prt, 0.1)
+    # the differentiable-area configuration at full size
+    res["differentiable_area_1M"] = differentiable_area(prt, 1_000_000)
+
     # small overlay configuration: 2 x 10,000 stars
     A = dg.star_layer(10000, seed=0)
     B = dg.star_layer(10000, seed=1)
@@ -425,6 +431,66 @@ def secondary(prt, boxes, flush, world):
                                              torch.arange(10000, device="cuda")))
     res["area_fwd_10k_pairs_s"] = 10000 / (ms * 1e-3)
     return res
+
+
+def differentiable_area(prt, n: int = 1_000_000, reps: int = 5):
+    """The differentiable intersection-area configuration: n overlapping pairs
+    of star polygons (16-64 vertices, float64; datagen.overlapping_pairs_device),
+    loss = sum of intersection areas.  Times (CUDA events, median of `reps`
+    after a warm-up) the forward (GPC clip + shoelace, area only) and the
+    backward adjoint kernel through the C ABI, and reports the backward
+    against the HBM roofline: algorithmic bytes = 32 B per vertex of both
+    polygons of every pair (16 B read, 16 B gradient written) + 16 B per pair
+    (ids and upstream gradient)."""
+    import ctypes as C
+
+    import torch
+    from parlllelrtree_b200 import _lib
+    from parlllelrtree_b200 import datagen as dg
+
+    A, B = dg.overlapping_pairs_device(n, seed=0)
+    LA, LB = prt.Layer.from_dict(A), prt.Layer.from_dict(B)
+    pa = torch.arange(n, dtype=torch.int32, device="cuda")
+    pb = pa.clone()
+    area = torch.empty(n, dtype=torch.float64, device="cuda")
+    up = torch.ones(n, dtype=torch.float64, device="cuda")
+    gb = torch.zeros_like(LA.xy)
+    go = torch.zeros_like(LB.xy)
+    sb, so = LA.struct(), LB.struct()
+    L = _lib.lib()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    p = lambda t: C.c_void_p(t.data_ptr())
+
+    def fwd():
+        _lib.check(L.prt_area_fwd(p(pa), p(pb), n, C.byref(sb), C.byref(so), p(area), st))
+
+    def bwd():
+        _lib.check(L.prt_area_bwd(p(pa), p(pb), n, C.byref(sb), C.byref(so), p(up), p(gb), p(go), st))
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(reps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return float(np.median(ms))
+
+    f_ms = timed(fwd)
+    b_ms = timed(bwd)
+    nv = int(len(LA.xy) + len(LB.xy))
+    algo = 32 * nv + 16 * n
+    peak, kind = hbm_peak()
+    achieved = algo / (b_ms * 1e-3) / 1e9
+    return {"pairs": n, "vertices": nv, "loss": float(area.sum()),
+            "fwd_ms": f_ms, "fwd_pairs_s": n / (f_ms * 1e-3), "bwd_ms": b_ms, "bwd_pairs_s": n / (b_ms * 1e-3),
+            "bwd_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_source": kind, "algorithmic_bytes": algo}}
 
 
 def batched_overlay(prt, scale: float = 1.0, reps: int = 1, pipeline: bool = True):

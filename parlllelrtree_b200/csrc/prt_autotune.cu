@@ -167,13 +167,13 @@ int prt_autotune(const prt_layer *base, const prt_layer *overlay, int op, int64_
     out->candidates++;
     return PRT_OK;
   };
-  int64_t warp_above = 64;
+  int64_t warp_above = 256;
   int slots = 128, wps = 8;
   prt_schedule best = make_schedule(warp_above, slots, wps);
   double best_ms = 1e30;
   if (!rc && m > 0) {
     rc = time_sched(best, &best_ms);
-    const int64_t cands_w[] = {0, 128, 256, 1024, 1ll << 41};
+    const int64_t cands_w[] = {0, 64, 1024, 1ll << 41};
     for (int64_t wa : cands_w) {
       if (rc || secs_since(t0) > time_budget_s) break;
       prt_schedule c = make_schedule(wa, slots, wps);

@@ -327,7 +327,7 @@ size_t arena_budget() {
 }  // namespace
 
 // ---- batched schedule ----------------------------------------------------------
-// Default: pairs above 64 vertices are clipped one per warp, smaller ones one
+// Default: pairs above 256 vertices are clipped one per warp, smaller ones one
 // per thread; 8 warps per SM, what an SM holds at the clip kernel's register
 // count.
 static prt_schedule default_schedule() {
@@ -337,7 +337,7 @@ static prt_schedule default_schedule() {
   d.aet_slots = 128;
   d.warps_per_sm = 8;
   const int64_t thr[5] = {1ll << 40, 4096, 1024, 256, 64};
-  const int32_t wm[5] = {1, 1, 1, 1, 0};
+  const int32_t wm[5] = {1, 1, 1, 0, 0};
   for (int b = 0; b < 5; b++) {
     d.bin_thresholds[b] = thr[b];
     d.bin_warp_mode[b] = wm[b];

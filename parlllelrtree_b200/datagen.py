@@ -255,7 +255,8 @@ def layer_bboxes(layer: dict) -> np.ndarray:
 
 def star_layer_device(n: int, seed: int, nv_lo: int = 4, nv_hi: int = 4096, r_lo: float = 1e-3,
                       r_hi: float = 1e-2, zipf: float | None = 1.2, hole_frac: float = 0.05,
-                      centres: str = "mixture", device: str = "cuda", chunk: int = 1 << 16) -> dict:
+                      centres: str = "mixture", device: str = "cuda", chunk: int = 1 << 16,
+                      centre_xy: np.ndarray | None = None, radii: np.ndarray | None = None) -> dict:
     """``star_layer`` for large layers: the per-polygon draws (vertex counts,
     radii, centres, holes, lobes) come from numpy, the per-vertex draws and
     trigonometry run in torch on ``device``, ``chunk`` polygons at a time so
@@ -269,8 +270,10 @@ def star_layer_device(n: int, seed: int, nv_lo: int = 4, nv_hi: int = 4096, r_lo
         nverts = np.clip(rng.zipf(zipf, size=n), nv_lo, nv_hi).astype(np.int64)
     else:
         nverts = rng.integers(nv_lo, nv_hi + 1, size=n).astype(np.int64)
-    radii = np.exp(rng.uniform(np.log(r_lo), np.log(r_hi), size=n))
-    centre_xy = mixture_centres(rng, n) if centres == "mixture" else rng.random((n, 2))
+    r_draw = np.exp(rng.uniform(np.log(r_lo), np.log(r_hi), size=n))
+    radii = r_draw if radii is None else np.asarray(radii, dtype=np.float64)
+    c_draw = mixture_centres(rng, n) if centres == "mixture" else rng.random((n, 2))
+    centre_xy = c_draw if centre_xy is None else np.asarray(centre_xy, dtype=np.float64)
     has_holes = rng.random(n) < hole_frac
     nholes = np.where(has_holes, rng.integers(1, 4, size=n), 0).astype(np.int64)
     amp = rng.random((n, 5))
@@ -341,3 +344,26 @@ def star_layer_device(n: int, seed: int, nv_lo: int = 4, nv_hi: int = 4096, r_lo
         del owner, k, p, hole_v, nv_p, theta, rr, h, sector, span, a0, m, frac, hang, rin, hr, ang, r_all, cen
     return {"poly_ring": torch.from_numpy(poly_ring).to(dev), "ring_vert": torch.from_numpy(ring_vert).to(dev),
             "ring_hole": torch.from_numpy((ring_j > 0).astype(np.int32)).to(dev), "xy": xy}
+
+
+def overlapping_pairs_device(n: int, seed: int = 0, nv_lo: int = 16, nv_hi: int = 64, r_lo: float = 1e-3,
+                             r_hi: float = 1e-2, device: str = "cuda"):
+    """The differentiable-area configuration: n pairs (A_i, B_i) of star
+    polygons with nv_lo..nv_hi vertices (uniform), float64, radius log-uniform
+    r_lo..r_hi, centres uniform in the unit square, no holes; B_i's centre is
+    A_i's moved by at most 0.5 r_A, inside the disk of radius 0.5 r_A that
+    every star contains, so each pair overlaps.  B_i's radius is r_A times
+    U(0.5, 1.5).  Returns the two layer dicts (torch, on ``device``); pair i
+    is (i, i)."""
+    rng = np.random.default_rng(seed + 424242)
+    cen = rng.random((n, 2))
+    ra = np.exp(rng.uniform(np.log(r_lo), np.log(r_hi), size=n))
+    ang = rng.uniform(0.0, 2.0 * np.pi, size=n)
+    dist = 0.5 * ra * np.sqrt(rng.random(n))
+    cb = cen + np.stack([dist * np.cos(ang), dist * np.sin(ang)], 1)
+    rb = ra * rng.uniform(0.5, 1.5, size=n)
+    A = star_layer_device(n, seed, nv_lo=nv_lo, nv_hi=nv_hi, zipf=None, hole_frac=0.0, device=device,
+                          centre_xy=cen, radii=ra)
+    B = star_layer_device(n, seed + 1, nv_lo=nv_lo, nv_hi=nv_hi, zipf=None, hole_frac=0.0, device=device,
+                          centre_xy=cb, radii=rb)
+    return A, B

@@ -25,12 +25,14 @@ def overlapping_pairs(n, seed, nv_lo=16, nv_hi=64, hole_frac=0.0):
     return A, B
 
 
-@pytest.mark.parametrize("hole_frac", [0.0, 0.5])
-def test_forward_and_adjoint_match_oracle(cuda, hole_frac):
+@pytest.mark.parametrize("hole_frac,nv", [(0.0, (16, 64)), (0.5, (16, 64)), (0.3, (100, 200))])
+def test_forward_and_adjoint_match_oracle(cuda, hole_frac, nv):
+    """Pairs of up to 128 vertices per polygon take the slab-indexed adjoint,
+    larger ones the brute-force one; both must give the oracle's gradient."""
     import parlllelrtree_b200 as prt
 
-    n = 2000
-    A, B = overlapping_pairs(n, seed=int(hole_frac * 10) + 1, hole_frac=hole_frac)
+    n = 2000 if nv[1] <= 64 else 300
+    A, B = overlapping_pairs(n, seed=int(hole_frac * 10) + nv[0], nv_lo=nv[0], nv_hi=nv[1], hole_frac=hole_frac)
     LA, LB = prt.Layer.from_dict(A), prt.Layer.from_dict(B)
     idx = torch.arange(n, dtype=torch.int32, device="cuda")
     xa = LA.xy.clone().requires_grad_(True)
