@@ -415,6 +415,8 @@ def secondary(prt, boxes, flush, world):
     res["uneven_overlay_0.1"] = batched_overlay(prt, 0.1)
     # the differentiable-area configuration at full size
     res["differentiable_area_1M"] = differentiable_area(prt, 1_000_000)
+    # the map-alignment loop, 200k parcels x 200 steps
+    res["alignment_200k"] = alignment(200_000)
 
     # small overlay configuration: 2 x 10,000 stars
     A = dg.star_layer(10000, seed=0)
@@ -491,6 +493,25 @@ def differentiable_area(prt, n: int = 1_000_000, reps: int = 5):
             "fwd_ms": f_ms, "fwd_pairs_s": n / (f_ms * 1e-3), "bwd_ms": b_ms, "bwd_pairs_s": n / (b_ms * 1e-3),
             "bwd_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_source": kind, "algorithmic_bytes": algo}}
+
+
+def alignment(n: int = 200_000):
+    """The map-alignment configuration: 200k parcels (jittered-grid hexagons
+    and quadrilaterals), the second layer under a random affine (rotation
+    +-2 deg, scale +-1%, translation +-0.005) plus vertex noise sigma 1e-4;
+    200 Adam steps, each rebuilding the R-tree, joining, clipping and running
+    the area adjoint (parlllelrtree_b200.alignment).  Reports steps/s from the
+    device time of the steps (CUDA events per pyramid stage) and the
+    recovery error."""
+    from parlllelrtree_b200 import alignment as al
+
+    A, B, T = al.parcel_layers(n, seed=3)
+    theta, rec, stage_s = al.fit_affine(A, B, steps=200)
+    total = sum(stage_s)
+    return {"parcels": n, "steps": len(rec), "device_s": total, "steps_s": len(rec) / total,
+            "stage_s": stage_s, "full_res_ms_per_step": stage_s[-1] / 50 * 1e3,
+            "recovery_error": al.recovery_error(theta, T), "initial_error": al.recovery_error(np.zeros(6), T),
+            "final_overlap": rec[-1]["overlap"]}
 
 
 def batched_overlay(prt, scale: float = 1.0, reps: int = 1, pipeline: bool = True):

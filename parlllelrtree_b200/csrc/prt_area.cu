@@ -358,8 +358,9 @@ extern "C" {
 
 int prt_area_fwd(const int32_t *d_pair_a, const int32_t *d_pair_b, int64_t n_pairs, const prt_layer *base,
                  const prt_layer *overlay, double *d_area, void *stream) {
-  PRT_CHECK(base && overlay && d_area && (n_pairs == 0 || (d_pair_a && d_pair_b)), PRT_ERR_INVALID,
+  PRT_CHECK(base && overlay && (n_pairs == 0 || (d_area && d_pair_a && d_pair_b)), PRT_ERR_INVALID,
             "NULL argument");
+  if (n_pairs == 0) return PRT_OK;
   PairSrc S;
   memset(&S, 0, sizeof S);
   S.pa = d_pair_a;
@@ -373,7 +374,7 @@ int prt_area_fwd(const int32_t *d_pair_a, const int32_t *d_pair_b, int64_t n_pai
 int prt_area_bwd(const int32_t *d_pair_a, const int32_t *d_pair_b, int64_t n_pairs, const prt_layer *base,
                  const prt_layer *overlay, const double *d_upstream, double *d_grad_base, double *d_grad_overlay,
                  void *stream) {
-  PRT_CHECK(base && overlay && d_grad_base && d_grad_overlay && (n_pairs == 0 || (d_pair_a && d_pair_b)),
+  PRT_CHECK(base && overlay && (n_pairs == 0 || (d_grad_base && d_grad_overlay && d_pair_a && d_pair_b)),
             PRT_ERR_INVALID, "NULL argument");
   if (n_pairs == 0) return PRT_OK;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
