@@ -5,7 +5,8 @@
 // same for all keys (they are skipped without a host round trip, so the whole
 // sort can be captured in a CUDA graph).  Each remaining pass is ONE kernel:
 // a CTA takes the next tile in launch order (atomic ticket), ranks its keys
-// with warp-level __match_any_sync multisplit, learns its global digit
+// with a warp-level multisplit (lanes with the same digit found by one ballot
+// per digit bit), learns its global digit
 // offsets by decoupled look-back over the preceding tiles (bounded spin, an
 // error flag instead of a hang), stages the tile in shared memory in digit
 // order and writes it out in coalesced runs.  Stable: ranks follow the
@@ -20,7 +21,7 @@ namespace {
 constexpr int kRadix = 256;
 constexpr int kSortBlock = 256;
 constexpr int kSortWarps = kSortBlock / 32;
-constexpr int kItems = 8;
+constexpr int kItems = 12;
 constexpr int kTile = kSortBlock * kItems;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
@@ -98,7 +99,7 @@ struct PassSmem {
   int tile;
 };
 
-constexpr int kLookBatch = 8;  // predecessor statuses read per look-back step
+constexpr int kLookBatch = 16;  // predecessor statuses read per look-back step
 
 template <typename KeyT>
 __global__ void __launch_bounds__(kSortBlock, 4) onesweep_pass(KeyT *keys0, uint32_t *vals0, KeyT *keys1,
@@ -154,14 +155,22 @@ __global__ void __launch_bounds__(kSortBlock, 4) onesweep_pass(KeyT *keys0, uint
   if (tile == 0) atomicExch(st, kFlagPrefix | ((goff[d] + total) & kCountMask));
   else atomicExch(st, kFlagAgg | (total & kCountMask));
 
-  // 2. stable ranks: warp multisplit with __match_any_sync
+  // 2. stable ranks: warp multisplit
   const uint32_t lt = lanemask_lt();
   uint32_t *wh = S.warp_hist[warp];
 #pragma unroll
   for (int i = 0; i < kItems; i++) {
     // lanes holding the same digit: the lowest one reads and bumps the warp's
     // counter for it, the others get the old count by shuffle
-    const uint32_t peers = __match_any_sync(0xffffffffu, dig[i]);
+    // lanes with the same 8-bit digit: AND of one ballot per digit bit
+    const bool ok = dig[i] < kRadix;
+    uint32_t peers = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+      const uint32_t m = __ballot_sync(0xffffffffu, (dig[i] >> b) & 1);
+      peers &= ((dig[i] >> b) & 1) ? m : ~m;
+    }
+    if (!ok) peers = 1u << lane;
     const int leader = __ffs(peers) - 1;
     uint32_t cnt = 0;
     if (lane == leader && dig[i] < kRadix) {
@@ -197,6 +206,17 @@ __global__ void __launch_bounds__(kSortBlock, 4) onesweep_pass(KeyT *keys0, uint
 #pragma unroll
   for (int w = 0; w < kSortWarps; w++) woff += w < warp ? S.scan_tmp[w] : 0u;
   S.digit_start[d] = woff + incl - total;
+  __syncthreads();
+  // stage the tile in digit order before the look-back: the items leave the
+  // registers, which the look-back's wide batches then use
+#pragma unroll
+  for (int i = 0; i < kItems; i++) {
+    if (dig[i] < kRadix) {
+      uint32_t pos = S.digit_start[dig[i]] + S.warp_hist[warp][dig[i]] + rank[i];
+      S.keys[pos] = k[i];
+      S.vals[pos] = v[i];
+    }
+  }
 
   // 3. decoupled look-back for digit d, kLookBatch predecessor statuses per
   //    round trip; every wait is bounded
@@ -236,25 +256,17 @@ __global__ void __launch_bounds__(kSortBlock, 4) onesweep_pass(KeyT *keys0, uint
     excl = acc;
     atomicExch(st, kFlagPrefix | ((excl + total) & kCountMask));
   }
-  S.global_start[d] = excl;
+  // staged position i of digit dd goes to global_start[dd] + i - digit_start[dd]
+  S.global_start[d] = excl - S.digit_start[d];
   __syncthreads();
 
-  // 4. stage in digit order, then write out in coalesced runs
-#pragma unroll
-  for (int i = 0; i < kItems; i++) {
-    if (dig[i] < kRadix) {
-      uint32_t pos = S.digit_start[dig[i]] + S.warp_hist[warp][dig[i]] + rank[i];
-      S.keys[pos] = k[i];
-      S.vals[pos] = v[i];
-    }
-  }
-  __syncthreads();
+  // 4. write the staged tile out in coalesced runs per digit
   int64_t valid = n - base;
   if (valid > kTile) valid = kTile;
   for (int i = tid; i < valid; i += kSortBlock) {
     KeyT kk = S.keys[i];
     int dd = (int)((kk >> shift) & 0xFF);
-    int64_t dst = (int64_t)S.global_start[dd] + (i - (int64_t)S.digit_start[dd]);
+    const uint32_t dst = S.global_start[dd] + (uint32_t)i;
     dst_k[dst] = kk;
     dst_v[dst] = S.vals[i];
   }
