@@ -514,6 +514,39 @@ def alignment(n: int = 200_000):
             "final_overlap": rec[-1]["overlap"]}
 
 
+def _cpu_overlay_sample(LA, LB, pairs, l2p, sample: int = 400, budget_s: float = 20.0):
+    """CPU baseline of the clip: the GPC restatement in oracle/ (C, one
+    thread) on an evenly strided sample of the candidate pairs, within a time
+    budget.  The reference's own CPU clip core (oracle/_ref) overflows its
+    fixed stack[400] on pairs with thousands of vertices, so the port stands
+    in for it here."""
+    import oracle
+
+    n = len(pairs)
+    step = max(1, n // sample)
+    idx = np.arange(0, n, step)[:sample]
+    p = pairs[idx].cpu().numpy()
+    perm = l2p.cpu().numpy()
+
+    def rings(L, i):
+        pr = L.poly_ring[i:i + 2].cpu().numpy()
+        rv = L.ring_vert[pr[0]:pr[1] + 1].cpu().numpy()
+        xy = L.xy[rv[0]:rv[-1]].cpu().numpy()
+        return [xy[rv[k] - rv[0]:rv[k + 1] - rv[0]] for k in range(len(rv) - 1)]
+
+    polys = [(rings(LA, int(perm[a])), rings(LB, int(b))) for a, b in p]
+    t0 = time.perf_counter()
+    done = 0
+    for s_, c_ in polys:
+        oracle.gpc_clip(s_, c_, 1)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "pairs/s", "cores": 1, "kind": "port",
+            "sample": f"{done} of {n} candidate pairs (every {step}th), GPC restatement in oracle/ (C), one thread"}
+
+
 def batched_overlay(prt, scale: float = 1.0, reps: int = 1, pipeline: bool = True):
     """The batched uneven overlay configuration: two layers of `scale` x 1M
     star polygons (vertex count clip(Zipf(1.2), 4, 4096), 5% with 1-3 clockwise
@@ -563,6 +596,7 @@ def batched_overlay(prt, scale: float = 1.0, reps: int = 1, pipeline: bool = Tru
         out[f"{sched}_pairs_s"] = len(pairs) / (best * 1e-3)
         out[f"{sched}_nonempty"], out[f"{sched}_retried"], out[f"{sched}_contours"], out[f"{sched}_vertices"] = info
     out["batched_over_plain"] = out["batched_pairs_s"] / out["plain_pairs_s"]
+    out["cpu_baseline"] = _cpu_overlay_sample(LA, LB, pairs, l2p)
     if pipeline:
         stream = torch.cuda.Stream()
         with torch.cuda.stream(stream):
