@@ -117,37 +117,63 @@ __device__ void pieces(const Poly &A, const Poly &B, double w, double *grad, int
 }
 
 // ---- shared-memory adjoint (pairs up to kBwdMaxV vertices per polygon) ----
-// The same boundary pieces with both polygons staged in shared memory.  Each
-// lane takes one edge (the edges of A and of B in one pass) and runs over the
-// edges of the other polygon in the same order as its neighbours, so the
-// loads are broadcasts and the lanes do not diverge.  A conservative float
-// bounding box (rounded outwards) rejects most edges before any double
-// arithmetic; the exact crossing expression runs only for the rest.  The
+// The same boundary pieces with both polygons staged in shared memory, and
+// the candidate edges of the other polygon found through y slabs instead of
+// a scan over all of its edges.  The pair's common y range (float, rounded
+// outwards) is cut into kSlabs slabs; slab s of polygon Q holds a bitmask of
+// Q's edges whose float box reaches slab s (built by a warp bit transpose of
+// each edge's slab range).  The slab index is a monotone function of the
+// float y, so two y ranges that overlap always share a slab and the masks
+// never drop a candidate:
+//   crossings of an edge: the OR of the slab masks over its y range, then the
+//     float box test and the exact FP64 crossing expression of
+//     next_crossing, so the crossing set equals the exhaustive scan's;
+//   midpoint of an interval: only edges whose y range holds the midpoint's y
+//     can straddle it, and they all sit in the midpoint's slab; the even-odd
+//     test is inside_evenodd's expression.
+// Each lane takes one edge (the edges of A and of B in one pass); the
 // crossing parameters are sorted and deduplicated, which gives the intervals
-// of next_crossing's repeated minimum search, and a second pass tests every
-// interval midpoint (inside_evenodd's expression, behind a float y-range
-// check).  Pairs with larger polygons, and edges with more than kBwdMaxT
-// crossings, take the global-memory path (pieces / next_crossing).
+// of next_crossing's repeated minimum search.  The two gradient contributions
+// a vertex receives (as the end of one edge, as the start of the next) are
+// summed across neighbouring lanes before the atomics.  Edges with more than
+// kBwdMaxT crossings take the global-memory path (next_crossing).
 constexpr int kBwdMaxV = 128;
 constexpr int kBwdMaxT = 16;
 constexpr int kBwdWarps = 4;
+constexpr int kSlabs = 32;
+constexpr unsigned kFullMask = 0xffffffffu;
 
 struct BwdPoly {  // one polygon in shared memory
-  float4 bb[kBwdMaxV];     // edge k's box (x_lo, y_lo, x_hi, y_hi), rounded outwards
+  float4 bb[kBwdMaxV];                    // edge k's box (x_lo, y_lo, x_hi, y_hi), rounded outwards
   double x[kBwdMaxV], y[kBwdMaxV];
-  int8_t sgn[kBwdMaxV];    // orientation sign of edge k (0: ring of < 2 vertices)
-  uint8_t nxt[kBwdMaxV];   // end vertex of edge k
+  uint32_t slab[kBwdMaxV / 32][kSlabs];  // word c of slab s: bit k = edge 32 c + k reaches slab s
+  int8_t sgn[kBwdMaxV];                   // orientation sign of edge k (0: ring of < 2 vertices)
+  uint8_t nxt[kBwdMaxV];                  // end vertex of edge k
+  uint8_t rst[kBwdMaxV];                  // first vertex of edge k's ring
+};
+
+// y -> slab: monotone non-decreasing in y (round-to-nearest float steps and a
+// clamp), which is what makes the slab masks conservative.
+struct SlabGrid {
+  float y0, scale;
+  __device__ int operator()(float y) const {
+    const float f = __fmul_rn(__fsub_rn(y, y0), scale);
+    return (int)fminf(fmaxf(f, 0.0f), (float)(kSlabs - 1));
+  }
 };
 
 // Loads a polygon into shared memory with its ring links, orientation signs
-// and edge boxes; returns its vertex count (all lanes).  Nothing is loaded
-// when the polygon has more than kBwdMaxV vertices.
-__device__ inline int bwd_load(const LayerDev &L, int64_t poly, BwdPoly &Q) {
+// and edge boxes; returns its vertex count (all lanes) and, in *ext, the
+// float extent of its edge boxes.  Nothing is loaded when the polygon has
+// more than kBwdMaxV vertices.
+__device__ inline int bwd_load(const LayerDev &L, int64_t poly, BwdPoly &Q, float4 *ext) {
   const int lane = threadIdx.x & 31;
   const int64_t r0 = L.poly_ring[poly], r1 = L.poly_ring[poly + 1];
   const int64_t vbase = L.ring_vert[r0];
   const int nv = (int)(L.ring_vert[r1] - vbase);
   if (nv > kBwdMaxV) return nv;
+  float4 e = make_float4(__int_as_float(0x7f800000), __int_as_float(0x7f800000), -__int_as_float(0x7f800000),
+                         -__int_as_float(0x7f800000));
   for (int64_t r = r0; r < r1; r++) {
     const int v0 = (int)(L.ring_vert[r] - vbase), n = (int)(L.ring_vert[r + 1] - L.ring_vert[r]);
     double sa = 0.0;
@@ -159,16 +185,54 @@ __device__ inline int bwd_load(const LayerDev &L, int64_t poly, BwdPoly &Q) {
       Q.x[v0 + i] = xi;
       Q.y[v0 + i] = yi;
       Q.nxt[v0 + i] = (uint8_t)(v0 + j);
-      Q.bb[v0 + i] = make_float4(__double2float_rd(fmin(xi, xj)), __double2float_rd(fmin(yi, yj)),
-                                 __double2float_ru(fmax(xi, xj)), __double2float_ru(fmax(yi, yj)));
+      Q.rst[v0 + i] = (uint8_t)v0;
+      const float4 b = make_float4(__double2float_rd(fmin(xi, xj)), __double2float_rd(fmin(yi, yj)),
+                                   __double2float_ru(fmax(xi, xj)), __double2float_ru(fmax(yi, yj)));
+      Q.bb[v0 + i] = b;
+      e = make_float4(fminf(e.x, b.x), fminf(e.y, b.y), fmaxf(e.z, b.z), fmaxf(e.w, b.w));
     }
-    for (int o = 16; o; o >>= 1) sa += __shfl_xor_sync(0xffffffffu, sa, o);
+    for (int o = 16; o; o >>= 1) sa += __shfl_xor_sync(kFullMask, sa, o);
     const bool hole = L.ring_hole && L.ring_hole[r];
     const int8_t sg = n < 2 ? 0 : (int8_t)((sa >= 0.0 ? 1 : -1) * (hole ? -1 : 1));
     for (int i = lane; i < n; i += 32) Q.sgn[v0 + i] = sg;
   }
+  for (int o = 16; o; o >>= 1) {
+    e.x = fminf(e.x, __shfl_xor_sync(kFullMask, e.x, o));
+    e.y = fminf(e.y, __shfl_xor_sync(kFullMask, e.y, o));
+    e.z = fmaxf(e.z, __shfl_xor_sync(kFullMask, e.z, o));
+    e.w = fmaxf(e.w, __shfl_xor_sync(kFullMask, e.w, o));
+  }
+  *ext = e;
   __syncwarp();
   return nv;
+}
+
+// 32 x 32 bit matrix transpose across the warp: bit i of lane l's result is
+// bit l of lane i's input (recursive exchange of off-diagonal blocks).
+__device__ inline uint32_t bit_transpose(uint32_t x) {
+  const int lane = threadIdx.x & 31;
+  uint32_t m = 0x0000ffffu;
+#pragma unroll
+  for (int j = 16; j; j >>= 1, m ^= m << j) {
+    const uint32_t t = __shfl_xor_sync(kFullMask, x, j);
+    x = (lane & j) ? ((x & ~m) | ((t >> j) & m)) : ((x & m) | ((t << j) & ~m));
+  }
+  return x;
+}
+
+// Slab masks of a staged polygon of nq edges.
+__device__ inline void bwd_slabs(BwdPoly &Q, int nq, const SlabGrid &g) {
+  const int lane = threadIdx.x & 31;
+  for (int c = 0; c < (nq + 31) / 32; c++) {
+    const int k = 32 * c + lane;
+    uint32_t row = 0;
+    if (k < nq) {
+      const float4 b = Q.bb[k];
+      row = (kFullMask >> (31 - g(b.w))) & (kFullMask << g(b.y));
+    }
+    Q.slab[c][lane] = bit_transpose(row);
+  }
+  __syncwarp();
 }
 
 // One edge whose crossings overflow the per-lane list: the global-memory path.
@@ -188,70 +252,122 @@ __device__ __noinline__ void bwd_edge_global(const Poly &Qg, double px, double p
   }
 }
 
+// Even-odd test of (mx, my) against staged polygon Q through the slab of
+// my: inside_evenodd's expression over the edges that can straddle my.
+__device__ inline bool bwd_inside(const BwdPoly &Q, int nwq, const float4 &qe, const SlabGrid &g, double mx,
+                                  double my) {
+  const float fy = __double2float_rn(my);
+  if (fy < qe.y || fy > qe.w) return false;  // no edge of Q straddles my
+  const int s = g(fy);
+  bool in = false;
+  for (int c = 0; c < nwq; c++) {
+    uint32_t bits = Q.slab[c][s];
+    while (bits) {
+      const int k = 32 * c + __ffs(bits) - 1;
+      bits &= bits - 1;
+      const int l = Q.nxt[k];
+      const double ay = Q.y[k], by = Q.y[l];
+      if ((ay > my) != (by > my)) {
+        const double ax = Q.x[k], bx = Q.x[l];
+        const double xi = ax + (my - ay) * (bx - ax) / (by - ay);
+        if (mx < xi) in = !in;
+      }
+    }
+  }
+  return in;
+}
+
+// Inside bits of the m + 1 intervals of an edge, each by its midpoint.
+__device__ __noinline__ unsigned bwd_midpoints(const BwdPoly &Q, int nwq, const float4 &qe, const SlabGrid &g,
+                                               double px, double py, double rx, double ry, const double *ts, int m) {
+  unsigned in = 0;
+  for (int a = 0; a <= m; a++) {
+    const double t0 = a == 0 ? 0.0 : ts[a - 1], t1 = a < m ? ts[a] : 1.0;
+    const double tm = 0.5 * (t0 + t1);
+    if (bwd_inside(Q, nwq, qe, g, px + tm * rx, py + tm * ry)) in |= 1u << a;
+  }
+  return in;
+}
+
 // pieces() for both polygons of a staged pair: lane edge e < na is edge e of
-// A (against B), e >= na edge e - na of B (against A).
-__device__ inline void bwd_pair(const BwdPoly *M, int na, int nb, double w, double *ga, double *gb, int64_t va,
-                                int64_t vb, const Poly &Ag, const Poly &Bg) {
+// A (against B), e >= na edge e - na of B (against A); rounds of 32 edges.
+// ext[0], ext[1]: the float extents of A and B.
+//
+// Which intervals are inside: the midpoint of each interval (the
+// definition), or, while the pair's crossings are all clean, by parity: a
+// ring's first interval by its midpoint, every later interval of the ring
+// flips at each crossing (prefix XOR of the crossing counts over the ring's
+// edges, carried between rounds).  A crossing is clean when it is well inside
+// both edges (t and u at least 1e-9 from 0 and 1), the edges are not nearly
+// parallel and no two crossings of an edge coincide; collinear overlapping
+// edges are not clean either.  From the first round with an unclean crossing
+// (or an edge past kBwdMaxT crossings) on, the pair uses midpoints.  Clean
+// crossings flip the inside state exactly where the midpoints change, so the
+// two give the same intervals.
+__device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int nb, const SlabGrid &g, double w,
+                                double *ga, double *gb, int64_t va, int64_t vb, const Poly &Ag, const Poly &Bg) {
   const int lane = threadIdx.x & 31;
-  const int nk = na > nb ? na : nb;
+  const unsigned lt = (1u << lane) - 1u;
+  bool mid = false;    // midpoint mode (sticky)
+  bool carry = false;  // parity mode: inside state after the last edge of the previous round
   for (int e0 = 0; e0 < na + nb; e0 += 32) {
     const int e = e0 + lane;
     const int side = e < na ? 0 : 1;
     const int i = side ? e - na : e;
     const BwdPoly &P = M[side], &Q = M[1 - side];
-    const int nq = side ? na : nb;
+    const int nwq = ((side ? na : nb) + 31) >> 5;
     const bool valid = e < na + nb && P.sgn[i] != 0;
+    const int j = valid ? P.nxt[i] : 0;
     double px = 0.0, py = 0.0, qx = 0.0, qy = 0.0;
+    float4 pb = make_float4(0.f, 0.f, 0.f, 0.f);
     if (valid) {
-      const int j = P.nxt[i];
       px = P.x[i];
       py = P.y[i];
       qx = P.x[j];
       qy = P.y[j];
+      pb = P.bb[i];
     }
     const double rx = qx - px, ry = qy - py;
-    const float fx0 = __double2float_rd(fmin(px, qx)), fy0 = __double2float_rd(fmin(py, qy));
-    const float fx1 = __double2float_ru(fmax(px, qx)), fy1 = __double2float_ru(fmax(py, qy));
-    // one uniform pass: candidate masks (bit k: edge k of Q) for crossings
-    // (boxes overlap) and for the midpoint tests (y ranges overlap)
-    unsigned mc[kBwdMaxV / 32], my[kBwdMaxV / 32];
-#pragma unroll
-    for (int c = 0; c < kBwdMaxV / 32; c++) {
-      unsigned wc = 0, wy = 0;
-      if (c * 32 < nk) {
-        for (int kk = 0; kk < 32; kk++) {
-          const int k = c * 32 + kk;
-          if (k >= nk) break;
-          const float4 b = Q.bb[k];
-          const bool yo = k < nq && !(b.w < fy0 || b.y > fy1);
-          const bool xo = !(b.z < fx0 || b.x > fx1);
-          wy |= (unsigned)yo << kk;
-          wc |= (unsigned)(yo && xo) << kk;
-        }
-      }
-      mc[c] = valid ? wc : 0u;
-      my[c] = valid ? wy : 0u;
-    }
     double ts[kBwdMaxT];
     int nt = 0;
-    bool over = false;
-#pragma unroll
-    for (int c = 0; c < kBwdMaxV / 32; c++) {
-      unsigned bits = mc[c];
-      while (bits) {
-        const int k = c * 32 + __ffs(bits) - 1;
-        bits &= bits - 1;
-        const int l = Q.nxt[k];
-        const double ax = Q.x[k], ay = Q.y[k], bx = Q.x[l], by = Q.y[l];
-        const double sx = bx - ax, sy = by - ay;
-        const double den = rx * sy - ry * sx;
-        if (den == 0.0) continue;
-        const double apx = ax - px, apy = ay - py;
-        const double t = (apx * sy - apy * sx) / den;
-        const double u = (apx * ry - apy * rx) / den;
-        if (t > 0.0 && t < 1.0 && u >= 0.0 && u <= 1.0) {
-          if (nt < kBwdMaxT) ts[nt++] = t;
-          else over = true;
+    bool over = false, unclean = false;
+    if (valid) {
+      const double rl = fabs(rx) + fabs(ry);
+      const int s0 = g(pb.y), s1 = g(pb.w);
+      for (int c = 0; c < nwq; c++) {
+        uint32_t bits = 0;
+        for (int s = s0; s <= s1; s++) bits |= Q.slab[c][s];
+        while (bits) {
+          const int k = 32 * c + __ffs(bits) - 1;
+          bits &= bits - 1;
+          const float4 b = Q.bb[k];
+          if (b.w < pb.y || b.y > pb.w || b.z < pb.x || b.x > pb.z) continue;
+          const int l = Q.nxt[k];
+          const double ax = Q.x[k], ay = Q.y[k], bx = Q.x[l], by = Q.y[l];
+          const double sx = bx - ax, sy = by - ay;
+          const double den = rx * sy - ry * sx;
+          const double apx = ax - px, apy = ay - py;
+          const double tn = apx * sy - apy * sx;
+          if (den == 0.0) {
+            unclean |= tn == 0.0;  // collinear
+            continue;
+          }
+          const double un = apx * ry - apy * rx;
+          // t = tn / den and u = un / den, with the signs of den folded in
+          const double d = fabs(den), tol = 1e-9 * d;
+          const double tt = den > 0.0 ? tn : -tn, uu = den > 0.0 ? un : -un;
+          if (tt < -tol || tt > d + tol || uu < -tol || uu > d + tol) continue;  // next_crossing rejects it
+          if (tt > tol && tt < d - tol && uu > tol && uu < d - tol && d > 1e-6 * rl * (fabs(sx) + fabs(sy))) {
+            if (nt < kBwdMaxT) ts[nt++] = tn / den;  // a clean crossing passes next_crossing's test
+            else over = true;
+            continue;
+          }
+          unclean = true;
+          const double t = tn / den, u = un / den;  // next_crossing's test
+          if (t > 0.0 && t < 1.0 && u >= 0.0 && u <= 1.0) {
+            if (nt < kBwdMaxT) ts[nt++] = t;
+            else over = true;
+          }
         }
       }
     }
@@ -267,53 +383,74 @@ __device__ inline void bwd_pair(const BwdPoly *M, int na, int nb, double w, doub
     int m = 0;
     for (int a = 0; a < nt; a++)
       if (m == 0 || ts[a] > ts[m - 1]) ts[m++] = ts[a];
+    unclean |= m != nt || over;
+    mid = __any_sync(kFullMask, unclean) || mid;
     // interval a = [b_a, b_{a+1}] with b_0 = 0, b_{m+1} = 1; bit a of `in`:
-    // its midpoint is inside the other polygon.  Every midpoint lies in the
-    // edge's y range, so only edges of Q overlapping that range can toggle.
-    const int nint = valid && !over ? m + 1 : 0;
+    // inside the other polygon
+    const float4 qe = ext[1 - side];
     unsigned in = 0;
-#pragma unroll
-    for (int c = 0; c < kBwdMaxV / 32; c++) {
-      unsigned bits = nint ? my[c] : 0u;
-      while (bits) {
-        const int k = c * 32 + __ffs(bits) - 1;
-        bits &= bits - 1;
-        const int l = Q.nxt[k];
-        const double ax = Q.x[k], ay = Q.y[k], bx = Q.x[l], by = Q.y[l];
-        for (int a = 0; a < nint; a++) {
-          const double t0 = a == 0 ? 0.0 : ts[a - 1], t1 = a < m ? ts[a] : 1.0;
-          const double tm = 0.5 * (t0 + t1);
-          const double mx = px + tm * rx, my2 = py + tm * ry;
-          if ((ay > my2) != (by > my2)) {
-            const double xi = ax + (my2 - ay) * (bx - ax) / (by - ay);
-            if (mx < xi) in ^= 1u << a;
-          }
-        }
+    if (mid) {
+      if (valid && !over) in = bwd_midpoints(Q, nwq, qe, g, px, py, rx, ry, ts, m);
+    } else {
+      const int rs = valid ? (side ? na : 0) + P.rst[i] : e;  // this edge's ring starts at edge rs
+      bool first = false;
+      if (valid && rs == e) {
+        const double tm = 0.5 * (m > 0 ? ts[0] : 1.0);
+        first = bwd_inside(Q, nwq, qe, g, px + tm * rx, py + tm * ry);
       }
+      const unsigned odd = __ballot_sync(kFullMask, (m & 1) != 0);
+      const int from = rs > e0 ? rs - e0 : 0;
+      const int par = __popc(odd & lt & ~((1u << from) - 1u)) & 1;
+      const bool sf = __shfl_sync(kFullMask, first, from);
+      const bool st = (rs >= e0 ? sf : carry) != (par != 0);  // inside state at the edge's start
+      in = (st ? 0x55555555u : 0xaaaaaaaau) & ((2u << m) - 1u);
+      carry = __shfl_sync(kFullMask, st != ((m & 1) != 0), 31);
     }
     double it = 0.0, i1 = 0.0;
     if (over) {
       bwd_edge_global(side ? Ag : Bg, px, py, rx, ry, &it, &i1);
     } else {
-      for (int a = 0; a < nint; a++) {
-        const double t0 = a == 0 ? 0.0 : ts[a - 1], t1 = a < m ? ts[a] : 1.0;
+      for (int a = 0; a <= m && valid; a++) {
         if ((in >> a) & 1u) {
+          const double t0 = a == 0 ? 0.0 : ts[a - 1], t1 = a < m ? ts[a] : 1.0;
           const double aa = 0.5 * (t1 * t1 - t0 * t0);
           it += aa;
           i1 += (t1 - t0) - aa;
         }
       }
     }
-    if (valid && (it != 0.0 || i1 != 0.0)) {
+    // contributions: it to the end vertex j, i1 to the start vertex i; the
+    // lane of the next edge of the ring hands its start contribution over so
+    // the shared vertex takes one atomic per coordinate
+    double gxj = 0.0, gyj = 0.0, gxi = 0.0, gyi = 0.0;
+    if (valid) {
       const double s = P.sgn[i];
-      const int j = P.nxt[i];
       const double nx = w * s * ry, ny = -w * s * rx;
-      double *g = side ? gb : ga;
-      const int64_t vbase = side ? vb : va;
-      atomicAdd(&g[2 * (vbase + j)], nx * it);
-      atomicAdd(&g[2 * (vbase + j) + 1], ny * it);
-      atomicAdd(&g[2 * (vbase + i)], nx * i1);
-      atomicAdd(&g[2 * (vbase + i) + 1], ny * i1);
+      gxj = nx * it;
+      gyj = ny * it;
+      gxi = nx * i1;
+      gyi = ny * i1;
+    }
+    const int key = valid ? (side << 8) | i : -1;           // this edge's start vertex
+    const int kend = valid ? (side << 8) | j : -2;          // its end vertex
+    const int knext = __shfl_down_sync(kFullMask, key, 1);  // start vertex of the next lane's edge
+    const int kprev = __shfl_up_sync(kFullMask, kend, 1);   // end vertex of the previous lane's edge
+    const double hx = __shfl_down_sync(kFullMask, gxi, 1), hy = __shfl_down_sync(kFullMask, gyi, 1);
+    const bool take = lane < 31 && knext == kend;  // the next lane's i1 part goes with mine
+    const bool given = lane > 0 && kprev == key;   // mine went to the previous lane
+    if (take) {
+      gxj += hx;
+      gyj += hy;
+    }
+    double *gr = side ? gb : ga;
+    const int64_t vbase = side ? vb : va;
+    if (valid && (gxj != 0.0 || gyj != 0.0)) {
+      atomicAdd(&gr[2 * (vbase + j)], gxj);
+      atomicAdd(&gr[2 * (vbase + j) + 1], gyj);
+    }
+    if (valid && !given && (gxi != 0.0 || gyi != 0.0)) {
+      atomicAdd(&gr[2 * (vbase + i)], gxi);
+      atomicAdd(&gr[2 * (vbase + i) + 1], gyi);
     }
   }
 }
@@ -338,17 +475,25 @@ __global__ void __launch_bounds__(32 * kBwdWarps) area_bwd_kernel(
     const double w = upstream ? upstream[i] : 1.0;
     Poly A{base.ring_vert, base.ring_hole, base.xy, base.poly_ring[a], base.poly_ring[a + 1]};
     Poly B{over.ring_vert, over.ring_hole, over.xy, over.poly_ring[b], over.poly_ring[b + 1]};
-    const int na = bwd_load(base, a, M[0]);
-    const int nb = bwd_load(over, b, M[1]);
+    float4 ext[2];
+    const int na = bwd_load(base, a, M[0], &ext[0]);
+    const int nb = bwd_load(over, b, M[1], &ext[1]);
     if (na <= kBwdMaxV && nb <= kBwdMaxV) {
-      bwd_pair(M, na, nb, w, grad_base, grad_over, base.ring_vert[A.r0], over.ring_vert[B.r0], A, B);
+      // boxes apart: no crossings and no midpoint inside the other polygon
+      const float y0 = fmaxf(ext[0].y, ext[1].y), y1 = fminf(ext[0].w, ext[1].w);
+      if (!(fmaxf(ext[0].x, ext[1].x) > fminf(ext[0].z, ext[1].z) || y0 > y1)) {
+        const float span = __fsub_rn(y1, y0);
+        const SlabGrid g{y0, span > 1e-30f ? __fdiv_rn((float)kSlabs, span) : 0.0f};
+        bwd_slabs(M[0], na, g);
+        bwd_slabs(M[1], nb, g);
+        bwd_pair(M, ext, na, nb, g, w, grad_base, grad_over, base.ring_vert[A.r0], over.ring_vert[B.r0], A, B);
+      }
     } else {
       bwd_pair_global(A, B, w, grad_base, grad_over);
     }
     __syncwarp();
   }
 }
-
 }  // namespace
 }  // namespace prt
 
