@@ -146,65 +146,113 @@ constexpr unsigned kFullMask = 0xffffffffu;
 struct BwdPoly {  // one polygon in shared memory
   float4 bb[kBwdMaxV];                    // edge k's box (x_lo, y_lo, x_hi, y_hi), rounded outwards
   double x[kBwdMaxV], y[kBwdMaxV];
-  uint32_t slab[kBwdMaxV / 32][kSlabs];  // word c of slab s: bit k = edge 32 c + k reaches slab s
+  uint32_t slab[kBwdMaxV / 32][kSlabs];   // y slabs: word c of slab s, bit k = edge 32 c + k reaches slab s
+  uint32_t xslab[kBwdMaxV / 32][kSlabs];  // the same for x slabs
+  int16_t ringv[33];                      // first vertex of ring r; ringv[rings] = the vertex count
   int8_t sgn[kBwdMaxV];                   // orientation sign of edge k (0: ring of < 2 vertices)
   uint8_t nxt[kBwdMaxV];                  // end vertex of edge k
   uint8_t rst[kBwdMaxV];                  // first vertex of edge k's ring
 };
 
-// y -> slab: monotone non-decreasing in y (round-to-nearest float steps and a
-// clamp), which is what makes the slab masks conservative.
+// coordinate -> slab: monotone non-decreasing (round-to-nearest float steps
+// and a clamp), which is what makes the slab masks conservative.
 struct SlabGrid {
-  float y0, scale;
-  __device__ int operator()(float y) const {
-    const float f = __fmul_rn(__fsub_rn(y, y0), scale);
+  float v0, scale;
+  __device__ int operator()(float v) const {
+    const float f = __fmul_rn(__fsub_rn(v, v0), scale);
     return (int)fminf(fmaxf(f, 0.0f), (float)(kSlabs - 1));
   }
 };
 
-// Loads a polygon into shared memory with its ring links, orientation signs
-// and edge boxes; returns its vertex count (all lanes) and, in *ext, the
-// float extent of its edge boxes.  Nothing is loaded when the polygon has
-// more than kBwdMaxV vertices.
-__device__ inline int bwd_load(const LayerDev &L, int64_t poly, BwdPoly &Q, float4 *ext) {
+__device__ inline SlabGrid slab_grid(float lo, float hi) {
+  const float span = __fsub_rn(hi, lo);
+  return SlabGrid{lo, span > 1e-30f ? __fdiv_rn((float)kSlabs, span) : 0.0f};
+}
+
+// Stages both polygons of a pair (A from rings [ra0, ra1) of LA, B from
+// [rb0, rb1) of LB) with their ring links, orientation signs and edge boxes;
+// the loads of the two are issued together.  nv[p] is polygon p's vertex
+// count, vb[p] its first vertex, ext[p] the float extent of its edge boxes.
+// Returns false (nothing staged) when a polygon has more than kBwdMaxV
+// vertices or more than 31 rings.
+__device__ inline bool bwd_load_pair(const LayerDev &LA, int64_t ra0, int64_t ra1, const LayerDev &LB, int64_t rb0,
+                                     int64_t rb1, BwdPoly *M, int *nv, int64_t *vb, float4 *ext) {
   const int lane = threadIdx.x & 31;
-  const int64_t r0 = L.poly_ring[poly], r1 = L.poly_ring[poly + 1];
-  const int64_t vbase = L.ring_vert[r0];
-  const int nv = (int)(L.ring_vert[r1] - vbase);
-  if (nv > kBwdMaxV) return nv;
-  float4 e = make_float4(__int_as_float(0x7f800000), __int_as_float(0x7f800000), -__int_as_float(0x7f800000),
-                         -__int_as_float(0x7f800000));
-  for (int64_t r = r0; r < r1; r++) {
-    const int v0 = (int)(L.ring_vert[r] - vbase), n = (int)(L.ring_vert[r + 1] - L.ring_vert[r]);
-    double sa = 0.0;
-    for (int i = lane; i < n; i += 32) {
-      const int j = (i + 1 == n) ? 0 : i + 1;
-      const double xi = L.xy[2 * (vbase + v0 + i)], yi = L.xy[2 * (vbase + v0 + i) + 1];
-      const double xj = L.xy[2 * (vbase + v0 + j)], yj = L.xy[2 * (vbase + v0 + j) + 1];
-      sa += xi * yj - xj * yi;
-      Q.x[v0 + i] = xi;
-      Q.y[v0 + i] = yi;
-      Q.nxt[v0 + i] = (uint8_t)(v0 + j);
-      Q.rst[v0 + i] = (uint8_t)v0;
-      const float4 b = make_float4(__double2float_rd(fmin(xi, xj)), __double2float_rd(fmin(yi, yj)),
-                                   __double2float_ru(fmax(xi, xj)), __double2float_ru(fmax(yi, yj)));
-      Q.bb[v0 + i] = b;
-      e = make_float4(fminf(e.x, b.x), fminf(e.y, b.y), fmaxf(e.z, b.z), fmaxf(e.w, b.w));
-    }
-    for (int o = 16; o; o >>= 1) sa += __shfl_xor_sync(kFullMask, sa, o);
-    const bool hole = L.ring_hole && L.ring_hole[r];
-    const int8_t sg = n < 2 ? 0 : (int8_t)((sa >= 0.0 ? 1 : -1) * (hole ? -1 : 1));
-    for (int i = lane; i < n; i += 32) Q.sgn[v0 + i] = sg;
+  const int nr[2] = {(int)(ra1 - ra0), (int)(rb1 - rb0)};
+  if (nr[0] > 31 || nr[1] > 31) return false;
+  int64_t rv[2] = {0, 0};
+  int hl[2] = {0, 0};
+  if (lane <= nr[0]) rv[0] = LA.ring_vert[ra0 + lane];
+  if (lane <= nr[1]) rv[1] = LB.ring_vert[rb0 + lane];
+  if (lane < nr[0] && LA.ring_hole) hl[0] = LA.ring_hole[ra0 + lane];
+  if (lane < nr[1] && LB.ring_hole) hl[1] = LB.ring_hole[rb0 + lane];
+#pragma unroll
+  for (int p = 0; p < 2; p++) {
+    vb[p] = __shfl_sync(kFullMask, rv[p], 0);
+    nv[p] = (int)(__shfl_sync(kFullMask, rv[p], nr[p]) - vb[p]);
   }
-  for (int o = 16; o; o >>= 1) {
-    e.x = fminf(e.x, __shfl_xor_sync(kFullMask, e.x, o));
-    e.y = fminf(e.y, __shfl_xor_sync(kFullMask, e.y, o));
-    e.z = fmaxf(e.z, __shfl_xor_sync(kFullMask, e.z, o));
-    e.w = fmaxf(e.w, __shfl_xor_sync(kFullMask, e.w, o));
-  }
-  *ext = e;
+  if (nv[0] > kBwdMaxV || nv[1] > kBwdMaxV) return false;
+#pragma unroll
+  for (int p = 0; p < 2; p++)
+    if (lane <= nr[p]) M[p].ringv[lane] = (int16_t)(rv[p] - vb[p]);
   __syncwarp();
-  return nv;
+  const float inf = __int_as_float(0x7f800000);
+  float4 e[2] = {make_float4(inf, inf, -inf, -inf), make_float4(inf, inf, -inf, -inf)};
+  double term[2][kBwdMaxV / 32];  // shoelace terms of this lane's vertices
+  int rix[2][kBwdMaxV / 32];      // and their rings
+#pragma unroll
+  for (int t = 0; t < kBwdMaxV / 32; t++) {
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+      const LayerDev &L = p ? LB : LA;
+      BwdPoly &Q = M[p];
+      const int i = 32 * t + lane;
+      term[p][t] = 0.0;
+      rix[p][t] = -1;
+      if (i < nv[p]) {
+        int r = 0;
+        while (Q.ringv[r + 1] <= i) r++;
+        const int v0 = Q.ringv[r], j = i + 1 == Q.ringv[r + 1] ? v0 : i + 1;
+        const double xi = L.xy[2 * (vb[p] + i)], yi = L.xy[2 * (vb[p] + i) + 1];
+        const double xj = L.xy[2 * (vb[p] + j)], yj = L.xy[2 * (vb[p] + j) + 1];
+        term[p][t] = xi * yj - xj * yi;
+        rix[p][t] = r;
+        Q.x[i] = xi;
+        Q.y[i] = yi;
+        Q.nxt[i] = (uint8_t)j;
+        Q.rst[i] = (uint8_t)v0;
+        const float4 b = make_float4(__double2float_rd(fmin(xi, xj)), __double2float_rd(fmin(yi, yj)),
+                                     __double2float_ru(fmax(xi, xj)), __double2float_ru(fmax(yi, yj)));
+        Q.bb[i] = b;
+        e[p] = make_float4(fminf(e[p].x, b.x), fminf(e[p].y, b.y), fmaxf(e[p].z, b.z), fmaxf(e[p].w, b.w));
+      }
+    }
+  }
+  // ring orientations: material on the left for CCW outer rings and CW holes
+#pragma unroll
+  for (int p = 0; p < 2; p++) {
+    for (int r = 0; r < nr[p]; r++) {
+      double sa = 0.0;
+#pragma unroll
+      for (int t = 0; t < kBwdMaxV / 32; t++) sa += rix[p][t] == r ? term[p][t] : 0.0;
+      for (int o = 16; o; o >>= 1) sa += __shfl_xor_sync(kFullMask, sa, o);
+      const bool hole = __shfl_sync(kFullMask, hl[p], r) != 0;
+      const int n = M[p].ringv[r + 1] - M[p].ringv[r];
+      const int8_t sg = n < 2 ? 0 : (int8_t)((sa >= 0.0 ? 1 : -1) * (hole ? -1 : 1));
+#pragma unroll
+      for (int t = 0; t < kBwdMaxV / 32; t++)
+        if (rix[p][t] == r) M[p].sgn[32 * t + lane] = sg;
+    }
+    for (int o = 16; o; o >>= 1) {
+      e[p].x = fminf(e[p].x, __shfl_xor_sync(kFullMask, e[p].x, o));
+      e[p].y = fminf(e[p].y, __shfl_xor_sync(kFullMask, e[p].y, o));
+      e[p].z = fmaxf(e[p].z, __shfl_xor_sync(kFullMask, e[p].z, o));
+      e[p].w = fmaxf(e[p].w, __shfl_xor_sync(kFullMask, e[p].w, o));
+    }
+    ext[p] = e[p];
+  }
+  __syncwarp();
+  return true;
 }
 
 // 32 x 32 bit matrix transpose across the warp: bit i of lane l's result is
@@ -220,17 +268,28 @@ __device__ inline uint32_t bit_transpose(uint32_t x) {
   return x;
 }
 
-// Slab masks of a staged polygon of nq edges.
-__device__ inline void bwd_slabs(BwdPoly &Q, int nq, const SlabGrid &g) {
+// y and x slab masks of both staged polygons (four independent transposes
+// per word).
+__device__ inline void bwd_slabs(BwdPoly *M, const int *nv, const SlabGrid &gy, const SlabGrid &gx) {
   const int lane = threadIdx.x & 31;
-  for (int c = 0; c < (nq + 31) / 32; c++) {
-    const int k = 32 * c + lane;
-    uint32_t row = 0;
-    if (k < nq) {
-      const float4 b = Q.bb[k];
-      row = (kFullMask >> (31 - g(b.w))) & (kFullMask << g(b.y));
+  const int nw = ((nv[0] > nv[1] ? nv[0] : nv[1]) + 31) / 32;
+  for (int c = 0; c < nw; c++) {
+    uint32_t ry[2], rx[2];
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+      const int k = 32 * c + lane;
+      ry[p] = rx[p] = 0;
+      if (k < nv[p]) {
+        const float4 b = M[p].bb[k];
+        ry[p] = (kFullMask >> (31 - gy(b.w))) & (kFullMask << gy(b.y));
+        rx[p] = (kFullMask >> (31 - gx(b.z))) & (kFullMask << gx(b.x));
+      }
     }
-    Q.slab[c][lane] = bit_transpose(row);
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+      M[p].slab[c][lane] = bit_transpose(ry[p]);
+      M[p].xslab[c][lane] = bit_transpose(rx[p]);
+    }
   }
   __syncwarp();
 }
@@ -304,7 +363,8 @@ __device__ __noinline__ unsigned bwd_midpoints(const BwdPoly &Q, int nwq, const 
 // (or an edge past kBwdMaxT crossings) on, the pair uses midpoints.  Clean
 // crossings flip the inside state exactly where the midpoints change, so the
 // two give the same intervals.
-__device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int nb, const SlabGrid &g, double w,
+__device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int nb, const SlabGrid &g,
+                                const SlabGrid &gx, double w,
                                 double *ga, double *gb, int64_t va, int64_t vb, const Poly &Ag, const Poly &Bg) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
@@ -333,10 +393,12 @@ __device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int
     bool over = false, unclean = false;
     if (valid) {
       const double rl = fabs(rx) + fabs(ry);
-      const int s0 = g(pb.y), s1 = g(pb.w);
+      const int s0 = g(pb.y), s1 = g(pb.w), x0 = gx(pb.x), x1 = gx(pb.z);
       for (int c = 0; c < nwq; c++) {
-        uint32_t bits = 0;
+        uint32_t bits = 0, xbits = 0;
         for (int s = s0; s <= s1; s++) bits |= Q.slab[c][s];
+        for (int s = x0; s <= x1; s++) xbits |= Q.xslab[c][s];
+        bits &= xbits;
         while (bits) {
           const int k = 32 * c + __ffs(bits) - 1;
           bits &= bits - 1;
@@ -393,10 +455,34 @@ __device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int
       if (valid && !over) in = bwd_midpoints(Q, nwq, qe, g, px, py, rx, ry, ts, m);
     } else {
       const int rs = valid ? (side ? na : 0) + P.rst[i] : e;  // this edge's ring starts at edge rs
-      bool first = false;
-      if (valid && rs == e) {
+      // the first interval of each ring starting in this round, by its
+      // midpoint: the whole warp tests it against all edges of the other polygon
+      const bool rstart = valid && rs == e;
+      double mx0 = 0.0, my0 = 0.0;
+      if (rstart) {
         const double tm = 0.5 * (m > 0 ? ts[0] : 1.0);
-        first = bwd_inside(Q, nwq, qe, g, px + tm * rx, py + tm * ry);
+        mx0 = px + tm * rx;
+        my0 = py + tm * ry;
+      }
+      bool first = false;
+      for (unsigned q = __ballot_sync(kFullMask, rstart); q; q &= q - 1) {
+        const int L = __ffs(q) - 1;
+        const double mxl = __shfl_sync(kFullMask, mx0, L), myl = __shfl_sync(kFullMask, my0, L);
+        const int sl = e0 + L < na ? 0 : 1;
+        const BwdPoly &QL = M[1 - sl];
+        const int nql = sl ? na : nb;
+        bool in = false;
+        for (int k = lane; k < nql; k += 32) {
+          const int l = QL.nxt[k];
+          const double ay = QL.y[k], by = QL.y[l];
+          if ((ay > myl) != (by > myl)) {
+            const double ax = QL.x[k], bx = QL.x[l];
+            const double xi = ax + (myl - ay) * (bx - ax) / (by - ay);
+            if (mxl < xi) in = !in;
+          }
+        }
+        const bool inside = (__popc(__ballot_sync(kFullMask, in)) & 1) != 0;
+        if (lane == L) first = inside;
       }
       const unsigned odd = __ballot_sync(kFullMask, (m & 1) != 0);
       const int from = rs > e0 ? rs - e0 : 0;
@@ -469,31 +555,69 @@ __global__ void __launch_bounds__(32 * kBwdWarps) area_bwd_kernel(
   BwdPoly *M = sm[threadIdx.x >> 5];
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t i = warp; i < n; i += nw) {
-    const int64_t a = pa[i], b = pb[i];
-    if (a < 0 || a >= base.n_poly || b < 0 || b >= over.n_poly) continue;
-    const double w = upstream ? upstream[i] : 1.0;
-    Poly A{base.ring_vert, base.ring_hole, base.xy, base.poly_ring[a], base.poly_ring[a + 1]};
-    Poly B{over.ring_vert, over.ring_hole, over.xy, over.poly_ring[b], over.poly_ring[b + 1]};
-    float4 ext[2];
-    const int na = bwd_load(base, a, M[0], &ext[0]);
-    const int nb = bwd_load(over, b, M[1], &ext[1]);
-    if (na <= kBwdMaxV && nb <= kBwdMaxV) {
-      // boxes apart: no crossings and no midpoint inside the other polygon
-      const float y0 = fmaxf(ext[0].y, ext[1].y), y1 = fminf(ext[0].w, ext[1].w);
-      if (!(fmaxf(ext[0].x, ext[1].x) > fminf(ext[0].z, ext[1].z) || y0 > y1)) {
-        const float span = __fsub_rn(y1, y0);
-        const SlabGrid g{y0, span > 1e-30f ? __fdiv_rn((float)kSlabs, span) : 0.0f};
-        bwd_slabs(M[0], na, g);
-        bwd_slabs(M[1], nb, g);
-        bwd_pair(M, ext, na, nb, g, w, grad_base, grad_over, base.ring_vert[A.r0], over.ring_vert[B.r0], A, B);
+  // a pair's ids are read one pair ahead and its ring ranges half a pair
+  // ahead, so the staging of a pair waits only for its ring starts and
+  // vertices
+  auto ids = [&](int64_t k, int64_t *a, int64_t *b) {
+    *a = -1;
+    *b = -1;
+    if (k < n) {
+      const int64_t x = pa[k], y = pb[k];
+      if (x >= 0 && x < base.n_poly && y >= 0 && y < over.n_poly) {
+        *a = x;
+        *b = y;
       }
-    } else {
-      bwd_pair_global(A, B, w, grad_base, grad_over);
     }
+  };
+  auto rings = [&](int64_t a, int64_t b, int64_t *r) {
+    r[0] = r[1] = r[2] = r[3] = 0;
+    if (a >= 0) {
+      r[0] = base.poly_ring[a];
+      r[1] = base.poly_ring[a + 1];
+      r[2] = over.poly_ring[b];
+      r[3] = over.poly_ring[b + 1];
+    }
+  };
+  int64_t a, b, rr[4];
+  ids(warp, &a, &b);
+  rings(a, b, rr);
+  for (int64_t i = warp; i < n; i += nw) {
+    int64_t an, bn, rn[4];
+    ids(i + nw, &an, &bn);
+    bool fetched = false;
+    if (a >= 0) {
+      const double w = upstream ? upstream[i] : 1.0;
+      int nv[2];
+      int64_t vb[2];
+      float4 ext[2];
+      const bool staged = bwd_load_pair(base, rr[0], rr[1], over, rr[2], rr[3], M, nv, vb, ext);
+      rings(an, bn, rn);
+      fetched = true;
+      if (staged) {
+        // boxes apart: no crossings and no midpoint inside the other polygon
+        const float x0 = fmaxf(ext[0].x, ext[1].x), x1 = fminf(ext[0].z, ext[1].z);
+        const float y0 = fmaxf(ext[0].y, ext[1].y), y1 = fminf(ext[0].w, ext[1].w);
+        if (!(x0 > x1 || y0 > y1)) {
+          const SlabGrid gy = slab_grid(y0, y1), gx = slab_grid(x0, x1);
+          bwd_slabs(M, nv, gy, gx);
+          Poly A{base.ring_vert, base.ring_hole, base.xy, rr[0], rr[1]};
+          Poly B{over.ring_vert, over.ring_hole, over.xy, rr[2], rr[3]};
+          bwd_pair(M, ext, nv[0], nv[1], gy, gx, w, grad_base, grad_over, vb[0], vb[1], A, B);
+        }
+      } else {
+        Poly A{base.ring_vert, base.ring_hole, base.xy, rr[0], rr[1]};
+        Poly B{over.ring_vert, over.ring_hole, over.xy, rr[2], rr[3]};
+        bwd_pair_global(A, B, w, grad_base, grad_over);
+      }
+    }
+    if (!fetched) rings(an, bn, rn);
+    a = an;
+    b = bn;
+    for (int k = 0; k < 4; k++) rr[k] = rn[k];
     __syncwarp();
   }
 }
+
 }  // namespace
 }  // namespace prt
 
