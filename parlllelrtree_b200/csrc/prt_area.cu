@@ -336,16 +336,74 @@ __device__ inline bool bwd_inside(const BwdPoly &Q, int nwq, const float4 &qe, c
   return in;
 }
 
-// Inside bits of the m + 1 intervals of an edge, each by its midpoint.
-__device__ __noinline__ unsigned bwd_midpoints(const BwdPoly &Q, int nwq, const float4 &qe, const SlabGrid &g,
-                                               double px, double py, double rx, double ry, const double *ts, int m) {
-  unsigned in = 0;
-  for (int a = 0; a <= m; a++) {
-    const double t0 = a == 0 ? 0.0 : ts[a - 1], t1 = a < m ? ts[a] : 1.0;
-    const double tm = 0.5 * (t0 + t1);
-    if (bwd_inside(Q, nwq, qe, g, px + tm * rx, py + tm * ry)) in |= 1u << a;
+// Candidate edges of Q (mask word c) for an edge whose box covers y slabs
+// [s0, s1] and x slabs [x0, x1].
+__device__ inline uint32_t bwd_cands(const BwdPoly &Q, int c, int s0, int s1, int x0, int x1) {
+  uint32_t ybits = 0, xbits = 0;
+  for (int s = s0; s <= s1; s++) ybits |= Q.slab[c][s];
+  for (int s = x0; s <= x1; s++) xbits |= Q.xslab[c][s];
+  return ybits & xbits;
+}
+
+// One edge p -> p + r against staged polygon Q by the definition: every
+// crossing by next_crossing's test (kBwdMaxT at most, else the global-memory
+// path), sorted and deduplicated, and every interval by its midpoint.
+__device__ __noinline__ void bwd_edge_exact(const BwdPoly &Q, int nwq, const float4 &qe, const SlabGrid &g,
+                                            const SlabGrid &gx, const float4 &pb, double px, double py, double rx,
+                                            double ry, const Poly &Qg, double *it_out, double *i1_out) {
+  double ts[kBwdMaxT];
+  int nt = 0;
+  bool over = false;
+  const int s0 = g(pb.y), s1 = g(pb.w), x0 = gx(pb.x), x1 = gx(pb.z);
+  for (int c = 0; c < nwq; c++) {
+    uint32_t bits = bwd_cands(Q, c, s0, s1, x0, x1);
+    while (bits) {
+      const int k = 32 * c + __ffs(bits) - 1;
+      bits &= bits - 1;
+      const float4 b = Q.bb[k];
+      if (b.w < pb.y || b.y > pb.w || b.z < pb.x || b.x > pb.z) continue;
+      const int l = Q.nxt[k];
+      const double ax = Q.x[k], ay = Q.y[k], bx = Q.x[l], by = Q.y[l];
+      const double sx = bx - ax, sy = by - ay;
+      const double den = rx * sy - ry * sx;
+      if (den == 0.0) continue;
+      const double apx = ax - px, apy = ay - py;
+      const double t = (apx * sy - apy * sx) / den;
+      const double u = (apx * ry - apy * rx) / den;
+      if (t > 0.0 && t < 1.0 && u >= 0.0 && u <= 1.0) {
+        if (nt < kBwdMaxT) ts[nt++] = t;
+        else over = true;
+      }
+    }
   }
-  return in;
+  double it = 0.0, i1 = 0.0;
+  if (over) {
+    bwd_edge_global(Qg, px, py, rx, ry, &it, &i1);
+  } else {
+    for (int a = 1; a < nt; a++) {  // sort, then drop duplicates
+      const double v = ts[a];
+      int b = a - 1;
+      while (b >= 0 && ts[b] > v) {
+        ts[b + 1] = ts[b];
+        b--;
+      }
+      ts[b + 1] = v;
+    }
+    int m = 0;
+    for (int a = 0; a < nt; a++)
+      if (m == 0 || ts[a] > ts[m - 1]) ts[m++] = ts[a];
+    for (int a = 0; a <= m; a++) {
+      const double t0 = a == 0 ? 0.0 : ts[a - 1], t1 = a < m ? ts[a] : 1.0;
+      const double tm = 0.5 * (t0 + t1);
+      if (bwd_inside(Q, nwq, qe, g, px + tm * rx, py + tm * ry)) {
+        const double aa = 0.5 * (t1 * t1 - t0 * t0);
+        it += aa;
+        i1 += (t1 - t0) - aa;
+      }
+    }
+  }
+  *it_out = it;
+  *i1_out = i1;
 }
 
 // pieces() for both polygons of a staged pair: lane edge e < na is edge e of
@@ -353,23 +411,26 @@ __device__ __noinline__ unsigned bwd_midpoints(const BwdPoly &Q, int nwq, const 
 // ext[0], ext[1]: the float extents of A and B.
 //
 // Which intervals are inside: the midpoint of each interval (the
-// definition), or, while the pair's crossings are all clean, by parity: a
-// ring's first interval by its midpoint, every later interval of the ring
-// flips at each crossing (prefix XOR of the crossing counts over the ring's
-// edges, carried between rounds).  A crossing is clean when it is well inside
-// both edges (t and u at least 1e-9 from 0 and 1), the edges are not nearly
-// parallel and no two crossings of an edge coincide; collinear overlapping
-// edges are not clean either.  From the first round with an unclean crossing
-// (or an edge past kBwdMaxT crossings) on, the pair uses midpoints.  Clean
-// crossings flip the inside state exactly where the midpoints change, so the
-// two give the same intervals.
+// definition, bwd_edge_exact), or, while the pair's crossings are all clean,
+// by parity: a ring's first interval by its midpoint, every later interval of
+// the ring flips at each crossing (prefix XOR of the crossing counts over the
+// ring's edges, carried between rounds).  A crossing is clean when it is well
+// inside both edges (t and u at least 1e-9 from 0 and 1) and the edges are
+// not nearly parallel; collinear overlapping edges, two coinciding crossings
+// on an edge and an edge with more than kBwdFast crossings are not clean.
+// From the first round with an unclean edge on, the pair goes by the
+// definition.  Clean crossings flip the inside state exactly where the
+// midpoints change and pass next_crossing's test, so the two give the same
+// intervals.  The clean path keeps an edge's crossings sorted in registers.
+constexpr int kBwdFast = 4;
+
 __device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int nb, const SlabGrid &g,
-                                const SlabGrid &gx, double w,
-                                double *ga, double *gb, int64_t va, int64_t vb, const Poly &Ag, const Poly &Bg) {
+                                const SlabGrid &gx, double w, double *ga, double *gb, int64_t va, int64_t vb,
+                                const Poly &Ag, const Poly &Bg) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
-  bool mid = false;    // midpoint mode (sticky)
-  bool carry = false;  // parity mode: inside state after the last edge of the previous round
+  bool exact = false;  // by the definition from here on (sticky)
+  bool carry = false;  // inside state after the last edge of the previous round
   for (int e0 = 0; e0 < na + nb; e0 += 32) {
     const int e = e0 + lane;
     const int side = e < na ? 0 : 1;
@@ -388,17 +449,15 @@ __device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int
       pb = P.bb[i];
     }
     const double rx = qx - px, ry = qy - py;
-    double ts[kBwdMaxT];
-    int nt = 0;
-    bool over = false, unclean = false;
-    if (valid) {
+    // clean crossings, ascending (2.0 = empty)
+    double t0c = 2.0, t1c = 2.0, t2c = 2.0, t3c = 2.0;
+    int m = 0;
+    bool unclean = false;
+    if (valid && !exact) {
       const double rl = fabs(rx) + fabs(ry);
       const int s0 = g(pb.y), s1 = g(pb.w), x0 = gx(pb.x), x1 = gx(pb.z);
       for (int c = 0; c < nwq; c++) {
-        uint32_t bits = 0, xbits = 0;
-        for (int s = s0; s <= s1; s++) bits |= Q.slab[c][s];
-        for (int s = x0; s <= x1; s++) xbits |= Q.xslab[c][s];
-        bits &= xbits;
+        uint32_t bits = bwd_cands(Q, c, s0, s1, x0, x1);
         while (bits) {
           const int k = 32 * c + __ffs(bits) - 1;
           bits &= bits - 1;
@@ -419,40 +478,27 @@ __device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int
           const double d = fabs(den), tol = 1e-9 * d;
           const double tt = den > 0.0 ? tn : -tn, uu = den > 0.0 ? un : -un;
           if (tt < -tol || tt > d + tol || uu < -tol || uu > d + tol) continue;  // next_crossing rejects it
-          if (tt > tol && tt < d - tol && uu > tol && uu < d - tol && d > 1e-6 * rl * (fabs(sx) + fabs(sy))) {
-            if (nt < kBwdMaxT) ts[nt++] = tn / den;  // a clean crossing passes next_crossing's test
-            else over = true;
+          if (!(tt > tol && tt < d - tol && uu > tol && uu < d - tol && d > 1e-6 * rl * (fabs(sx) + fabs(sy))) ||
+              m == kBwdFast) {
+            unclean = true;
             continue;
           }
-          unclean = true;
-          const double t = tn / den, u = un / den;  // next_crossing's test
-          if (t > 0.0 && t < 1.0 && u >= 0.0 && u <= 1.0) {
-            if (nt < kBwdMaxT) ts[nt++] = t;
-            else over = true;
-          }
+          double v = (apx * sy - apy * sx) / den;  // next_crossing's t
+          // sorted insert into the register list
+          if (v < t0c) { const double x = t0c; t0c = v; v = x; }
+          if (v < t1c) { const double x = t1c; t1c = v; v = x; }
+          if (v < t2c) { const double x = t2c; t2c = v; v = x; }
+          if (v < t3c) { const double x = t3c; t3c = v; v = x; }
+          m++;
         }
       }
+      unclean |= (m > 1 && t0c == t1c) || (m > 2 && t1c == t2c) || (m > 3 && t2c == t3c);
     }
-    for (int a = 1; a < nt; a++) {  // sort, then drop duplicates
-      const double v = ts[a];
-      int b = a - 1;
-      while (b >= 0 && ts[b] > v) {
-        ts[b + 1] = ts[b];
-        b--;
-      }
-      ts[b + 1] = v;
-    }
-    int m = 0;
-    for (int a = 0; a < nt; a++)
-      if (m == 0 || ts[a] > ts[m - 1]) ts[m++] = ts[a];
-    unclean |= m != nt || over;
-    mid = __any_sync(kFullMask, unclean) || mid;
-    // interval a = [b_a, b_{a+1}] with b_0 = 0, b_{m+1} = 1; bit a of `in`:
-    // inside the other polygon
-    const float4 qe = ext[1 - side];
-    unsigned in = 0;
-    if (mid) {
-      if (valid && !over) in = bwd_midpoints(Q, nwq, qe, g, px, py, rx, ry, ts, m);
+    exact = __any_sync(kFullMask, unclean) || exact;
+    double it = 0.0, i1 = 0.0;
+    if (exact) {
+      if (valid)
+        bwd_edge_exact(Q, nwq, ext[1 - side], g, gx, pb, px, py, rx, ry, side ? Ag : Bg, &it, &i1);
     } else {
       const int rs = valid ? (side ? na : 0) + P.rst[i] : e;  // this edge's ring starts at edge rs
       // the first interval of each ring starting in this round, by its
@@ -460,7 +506,7 @@ __device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int
       const bool rstart = valid && rs == e;
       double mx0 = 0.0, my0 = 0.0;
       if (rstart) {
-        const double tm = 0.5 * (m > 0 ? ts[0] : 1.0);
+        const double tm = 0.5 * (m > 0 ? t0c : 1.0);
         mx0 = px + tm * rx;
         my0 = py + tm * ry;
       }
@@ -489,19 +535,23 @@ __device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int
       const int par = __popc(odd & lt & ~((1u << from) - 1u)) & 1;
       const bool sf = __shfl_sync(kFullMask, first, from);
       const bool st = (rs >= e0 ? sf : carry) != (par != 0);  // inside state at the edge's start
-      in = (st ? 0x55555555u : 0xaaaaaaaau) & ((2u << m) - 1u);
       carry = __shfl_sync(kFullMask, st != ((m & 1) != 0), 31);
-    }
-    double it = 0.0, i1 = 0.0;
-    if (over) {
-      bwd_edge_global(side ? Ag : Bg, px, py, rx, ry, &it, &i1);
-    } else {
-      for (int a = 0; a <= m && valid; a++) {
-        if ((in >> a) & 1u) {
-          const double t0 = a == 0 ? 0.0 : ts[a - 1], t1 = a < m ? ts[a] : 1.0;
-          const double aa = 0.5 * (t1 * t1 - t0 * t0);
-          it += aa;
-          i1 += (t1 - t0) - aa;
+      // intervals [0, t0c], [t0c, t1c], ..., [t_{m-1}, 1], alternately inside
+      if (valid) {
+        bool in = st;
+        double a0 = 0.0;
+#pragma unroll
+        for (int a = 0; a <= kBwdFast; a++) {
+          if (a <= m) {
+            const double a1 = a < m ? (a == 0 ? t0c : a == 1 ? t1c : a == 2 ? t2c : t3c) : 1.0;
+            if (in) {
+              const double aa = 0.5 * (a1 * a1 - a0 * a0);
+              it += aa;
+              i1 += (a1 - a0) - aa;
+            }
+            a0 = a1;
+            in = !in;
+          }
         }
       }
     }
@@ -548,7 +598,9 @@ __device__ __noinline__ void bwd_pair_global(const Poly &A, const Poly &B, doubl
   pieces(B, A, w, gb, lane);
 }
 
-__global__ void __launch_bounds__(32 * kBwdWarps) area_bwd_kernel(
+// 4 blocks of 4 warps per SM: 120 registers, no spills (5 blocks would cap
+// the kernel at 96 registers and spill)
+__global__ void __launch_bounds__(32 * kBwdWarps, 4) area_bwd_kernel(
     const int32_t *__restrict__ pa, const int32_t *__restrict__ pb, int64_t n, LayerDev base, LayerDev over,
     const double *__restrict__ upstream, double *grad_base, double *grad_over) {
   __shared__ BwdPoly sm[kBwdWarps][2];
