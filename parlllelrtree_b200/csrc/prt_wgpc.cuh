@@ -585,6 +585,474 @@ __device__ inline int hstate_after(int carry, unsigned m1, unsigned m2, int x) {
   return (__popc(between) & 1) ? 3 - from : from;
 }
 
+// GPC's output step for one contributing slot (GPC:425-570), on one lane:
+// vertex class from the slot's flags, xb its bottom x; oa / ob are the
+// slot's above / below output polygons, cf the current fragment.  A contour
+// merge returns in rt the proxy to redirect and in rto its replacement.
+__device__ inline void wout_event(Arena &A, const WPoly &P, uint32_t fl, double xb, double yb, int &oa, int &ob, int &cf,
+                                  int &out_poly, int &rt, int &rto) {
+  const int vclass = (int)((fl >> W_VC) & 15u);
+  const bool pxne = (fl & W_PXNE) != 0;
+  switch (vclass) {
+    case EMN:
+    case IMN: {
+      const int k = wp_local_min(A, P, out_poly, xb, yb);
+      if (k >= 0) oa = k;
+      cf = oa;
+      break;
+    }
+    case ERI:
+      if (pxne) wp_add_right(A, P, cf, xb, yb);
+      oa = cf;
+      cf = -1;
+      break;
+    case ELI:
+      wp_add_left(A, P, ob, xb, yb);
+      cf = ob;
+      break;
+    case EMX:
+      if (pxne) wp_add_left(A, P, cf, xb, yb);
+      rt = wp_merge_right(A, P, cf, ob, &rto);
+      cf = -1;
+      break;
+    case ILI:
+      if (pxne) wp_add_left(A, P, cf, xb, yb);
+      oa = cf;
+      cf = -1;
+      break;
+    case IRI:
+      wp_add_right(A, P, ob, xb, yb);
+      cf = ob;
+      ob = -1;
+      break;
+    case IMX:
+      if (pxne) wp_add_right(A, P, cf, xb, yb);
+      rt = wp_merge_left(A, P, cf, ob, &rto);
+      cf = -1;
+      ob = -1;
+      break;
+    case IMM: {
+      if (pxne) wp_add_right(A, P, cf, xb, yb);
+      rt = wp_merge_left(A, P, cf, ob, &rto);
+      ob = -1;
+      const int k = wp_local_min(A, P, out_poly, xb, yb);
+      if (k >= 0) oa = k;
+      cf = oa;
+      break;
+    }
+    case EMM: {
+      if (pxne) wp_add_left(A, P, cf, xb, yb);
+      rt = wp_merge_right(A, P, cf, ob, &rto);
+      ob = -1;
+      const int k = wp_local_min(A, P, out_poly, xb, yb);
+      if (k >= 0) oa = k;
+      cf = oa;
+      break;
+    }
+    case LED:
+      if (fl & W_STARTS) wp_add_left(A, P, ob, xb, yb);
+      oa = ob;
+      break;
+    case RED:
+      if (fl & W_STARTS) wp_add_right(A, P, ob, xb, yb);
+      oa = ob;
+      break;
+    default:
+      break;
+  }
+}
+
+// Bundle fix-ups of deleted bundle heads (GPC:426-459), in AET order, on one
+// lane.
+__device__ inline void wfixups(const WAet &W, int n, double yb) {
+  for (int d = 0; d < n; d++) {
+    if (!(W.ty()[d] == yb && fbits(W.fl()[d], W_STB) == BUNDLE_HEAD)) continue;
+    int pe = d - 1;
+    while (pe >= 0 && W.ty()[pe] == yb) pe--;
+    if (pe < 0) continue;
+    if (fbits(W.fl()[pe], W_STB) == BUNDLE_TAIL) {
+      W.outB()[pe] = W.outB()[d];
+      W.fl()[pe] = fset(W.fl()[pe], W_STB, UNBUNDLED);
+      int pp = pe - 1;
+      while (pp >= 0 && W.ty()[pp] == yb) pp--;
+      if (pp >= 0 && fbits(W.fl()[pp], W_STB) == BUNDLE_TAIL) W.fl()[pe] = fset(W.fl()[pe], W_STB, BUNDLE_HEAD);
+    }
+  }
+}
+
+// A beam with intersections (GPC:461-659): the slots are spilled to the
+// linked form, the thread clipper's intersect_beam runs on lane 0 and the
+// slots are rebuilt in the new AET order.  Returns nonzero (A.status set, or
+// *mode = kWarpFallback for an AET list it leaves malformed) on failure.
+__device__ __noinline__ int wintersect(Arena &A, const WAet &W, const WPoly &P, int op, int n, double yb, double dy,
+                                       int &out_poly, int *mode) {
+  const int lane = threadIdx.x & 31;
+  for (int c = 0; c < n; c += 32) {
+    const int s = c + lane;
+    if (s < n) wspill(A, wload(W, s), s > 0 ? W.edge()[s - 1] : -1, s + 1 < n ? W.edge()[s + 1] : -1);
+  }
+  __syncwarp();
+  wp_sync(P, A.np, 0);
+  int bad = 0;
+  if (lane == 0) {
+    int aet = W.edge()[0];
+    intersect_beam(A, op, aet, out_poly, yb, dy);
+    if (!A.status) {
+      int cur = aet, k = 0;
+      while (cur >= 0 && k < n) {
+        W.ord()[k++] = cur;
+        cur = A.E[cur].next;
+      }
+      bad = (k != n || cur >= 0) ? 1 : 0;
+    }
+  }
+  __syncwarp();
+  A.status = __shfl_sync(kFull, A.status, 0);
+  out_poly = __shfl_sync(kFull, out_poly, 0);
+  bad = __shfl_sync(kFull, bad, 0);
+  wp_sync(P, A.np, 1);
+  if (bad) {
+    *mode = kWarpFallback;
+    return 1;
+  }
+  if (A.status) return 1;
+  for (int c = 0; c < n; c += 32) {
+    const int s = c + lane;
+    WSlot v;
+    if (s < n) v = wslot_of(A, W.ord()[s]);
+    __syncwarp();
+    if (s < n) wstore(W, s, v);
+  }
+  __syncwarp();
+  return 0;
+}
+
+// All fields of lane src's slot (wshfl) or of the lane below (wshfl_up).
+__device__ inline WSlot wshfl(const WSlot &v, int src) {
+  WSlot r;
+  r.xb = __shfl_sync(kFull, v.xb, src);
+  r.xt = __shfl_sync(kFull, v.xt, src);
+  r.dx = __shfl_sync(kFull, v.dx, src);
+  r.ty = __shfl_sync(kFull, v.ty, src);
+  r.bx = __shfl_sync(kFull, v.bx, src);
+  r.by = __shfl_sync(kFull, v.by, src);
+  r.tx = __shfl_sync(kFull, v.tx, src);
+  r.edge = __shfl_sync(kFull, v.edge, src);
+  r.outA = __shfl_sync(kFull, v.outA, src);
+  r.outB = __shfl_sync(kFull, v.outB, src);
+  r.succ = __shfl_sync(kFull, v.succ, src);
+  r.fl = __shfl_sync(kFull, v.fl, src);
+  return r;
+}
+
+__device__ inline WSlot wshfl_up(const WSlot &v) {
+  WSlot r;
+  r.xb = __shfl_up_sync(kFull, v.xb, 1);
+  r.xt = __shfl_up_sync(kFull, v.xt, 1);
+  r.dx = __shfl_up_sync(kFull, v.dx, 1);
+  r.ty = __shfl_up_sync(kFull, v.ty, 1);
+  r.bx = __shfl_up_sync(kFull, v.bx, 1);
+  r.by = __shfl_up_sync(kFull, v.by, 1);
+  r.tx = __shfl_up_sync(kFull, v.tx, 1);
+  r.edge = __shfl_up_sync(kFull, v.edge, 1);
+  r.outA = __shfl_up_sync(kFull, v.outA, 1);
+  r.outB = __shfl_up_sync(kFull, v.outB, 1);
+  r.succ = __shfl_up_sync(kFull, v.succ, 1);
+  r.fl = __shfl_up_sync(kFull, v.fl, 1);
+  return r;
+}
+
+// Position of the k-th (0-based) set bit of m; m has more than k set bits.
+__device__ inline int nth_bit(unsigned m, int k) {
+  int pos = 0;
+#pragma unroll
+  for (int w = 16; w; w >>= 1) {
+    const unsigned lo = m & ((1u << w) - 1u);
+    const int c = __popc(lo);
+    if (k >= c) {
+      k -= c;
+      m >>= w;
+      pos += w;
+    } else {
+      m = lo;
+    }
+  }
+  return pos;
+}
+
+// Beam-loop state handed between the shared-memory and the register loops.
+struct WBeams {
+  double yb, yt, dy, bwin;
+  int n, lmin, cf, out_poly, bbase;
+};
+
+enum : int { kBeamsDone = 0, kBeamsGrow = 1, kBeamsFail = -1 };
+
+// The scanbeam loop while the AET has at most 32 edges: slot k lives in the
+// registers of lane k, so every per-slot step of the shared-memory loop in
+// wclip_impl (the same steps, for one chunk of 32) runs on registers, with
+// ballots and shuffles for the neighbours.  The loop starts at a beam's
+// insertion step with the slots in W.  Returns kBeamsDone after the last
+// beam, kBeamsFail on failure (A.status or *mode set), and kBeamsGrow when an
+// insertion would make a 33rd slot: the slots are then back in W and the
+// shared-memory loop goes on with the same insertion.
+template <int op>
+__device__ __noinline__ int wbeams_reg(Arena &A, const WAet &W, const WPoly &P, WBeams &S, int *mode) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = lanemask_lt();
+  const int pC0 = op == OP_DIFF ? RIGHT : LEFT;
+  int n = S.n, lmin = S.lmin, cf = S.cf, out_poly = S.out_poly, bbase = S.bbase;
+  double yb = S.yb, yt = S.yt, dy = S.dy, bwin = S.bwin;
+  auto bys = [&](int i) -> double {
+    if (i - bbase >= 32) {
+      bbase += 32 * ((i - bbase) / 32);
+      bwin = bbase + lane < A.nb ? A.B[bbase + lane].y : 0.0;
+    }
+    return __shfl_sync(kFull, bwin, i - bbase);
+  };
+  WSlot R;
+  if (lane < n) R = wload(W, lane);
+  int ret = kBeamsDone;
+  for (;;) {
+    // ---- local minima at yb into the AET
+    bool grow = false;
+    while (lmin < A.nb && bys(lmin) == yb) {
+      if (n == 32) {
+        grow = true;
+        break;
+      }
+      const WSlot ns = wslot_of(A, A.B[lmin++].edge);
+      const unsigned m = __ballot_sync(kFull, lane < n && (ns.xb < R.xb || (ns.xb == R.xb && ns.dx < R.dx)));
+      const int pos = m ? __ffs(m) - 1 : n;
+      const WSlot up = wshfl_up(R);
+      if (lane > pos) R = up;
+      if (lane == pos) R = ns;
+      n++;
+    }
+    if (grow) {
+      wstore(W, lane, R);
+      __syncwarp();
+      ret = kBeamsGrow;
+      break;
+    }
+    if (n == 0) {
+      if (lmin >= A.nb) break;
+      yb = bys(lmin);
+      continue;
+    }
+    const bool valid = lane < n;
+
+    // ---- bundles above yb
+    {
+      const bool f = valid && R.ty != yb;
+      const unsigned mf = __ballot_sync(kFull, f);
+      const unsigned lower = mf & lt;
+      const int pj = lower ? 31 - __clz(lower) : lane;
+      const double pxb = __shfl_sync(kFull, R.xb, pj), pdx = __shfl_sync(kFull, R.dx, pj);
+      const bool link = f && lower && fabs(pxb - R.xb) <= kEps && fabs(pdx - R.dx) <= kEps;
+      const unsigned ml = __ballot_sync(kFull, link);
+      int acc = f ? (1 << (R.fl & W_TYPE)) : 0;
+      if (ml) {
+        int ptr = link ? pj : -1;
+        for (int d = 0; d < 5; d++) {
+          const int src = ptr >= 0 ? ptr : lane;
+          const int a2 = __shfl_sync(kFull, acc, src);
+          const int p2 = __shfl_sync(kFull, ptr, src);
+          if (ptr >= 0) {
+            acc ^= a2;
+            ptr = p2;
+          }
+        }
+      }
+      const unsigned upper = mf & ~lt & ~(1u << lane);
+      const int nj = upper ? __ffs(upper) - 1 : -1;
+      const bool tail = f && nj >= 0 && ((ml >> nj) & 1u);
+      if (valid) {
+        int ba, st;
+        if (tail) {
+          ba = 0;
+          st = BUNDLE_TAIL;
+        } else if (link) {
+          ba = acc;
+          st = BUNDLE_HEAD;
+        } else {
+          ba = acc;
+          st = UNBUNDLED;
+        }
+        R.fl = fset(fset(R.fl, W_BA, ba), W_STA, st);
+      }
+    }
+
+    // ---- parity, horizontal state, vertex classes
+    unsigned mc;
+    bool any_fix;
+    {
+      uint32_t fl = valid ? R.fl : 0u;
+      const int ba = fbits(fl, W_BA), bb = fbits(fl, W_BB);
+      const int aC = ba & 1, aS = ba >> 1, bC = bb & 1, bS = bb >> 1;
+      const int exC = aC + (bC << 1), exS = aS + (bS << 1);
+      const unsigned maC = __ballot_sync(kFull, aC), maS = __ballot_sync(kFull, aS);
+      const int pCb = pC0 ^ (__popc(maC & lt) & 1), pSb = LEFT ^ (__popc(maS & lt) & 1);
+      const int pCa = pCb ^ aC, pSa = pSb ^ aS;
+      const unsigned m1C = __ballot_sync(kFull, exC == 1 || exC == 2), m2C = __ballot_sync(kFull, exC == 3);
+      const unsigned m1S = __ballot_sync(kFull, exS == 1 || exS == 2), m2S = __ballot_sync(kFull, exS == 3);
+      const int xC = ((exC == 2) ^ pCa) ? TH : BH, xS = ((exS == 2) ^ pSa) ? TH : BH;
+      const int horC = hstate_before(NH, m1C, m2C, xC), horS = hstate_before(NH, m1S, m2S, xS);
+      const bool exists = valid && (exC || exS);
+      bool contributing = false;
+      int vclass = 0;
+      if (exists) {
+        const int hc = horC != NH, hs = horS != NH;
+        int br = 0, bl = 0, tr = 0, tl = 0;
+        if (op == OP_DIFF || op == OP_INT) {
+          contributing = (exC && (pSb || horS)) || (exS && (pCb || horC)) || (exC && exS && (pCb == pSb));
+          br = pCb && pSb;
+          bl = (pCb ^ aC) && (pSb ^ aS);
+          tr = (pCb ^ hc) && (pSb ^ hs);
+          tl = (pCb ^ hc ^ bC) && (pSb ^ hs ^ bS);
+        } else if (op == OP_XOR) {
+          contributing = exC || exS;
+          br = pCb ^ pSb;
+          bl = (pCb ^ aC) ^ (pSb ^ aS);
+          tr = (pCb ^ hc) ^ (pSb ^ hs);
+          tl = (pCb ^ hc ^ bC) ^ (pSb ^ hs ^ bS);
+        } else {
+          contributing = (exC && (!pSb || horS)) || (exS && (!pCb || horC)) || (exC && exS && (pCb == pSb));
+          br = pCb || pSb;
+          bl = (pCb ^ aC) || (pSb ^ aS);
+          tr = (pCb ^ hc) || (pSb ^ hs);
+          tl = (pCb ^ hc ^ bC) || (pSb ^ hs ^ bS);
+        }
+        vclass = tr + (tl << 1) + (br << 2) + (bl << 3);
+        fl = fset(fl, W_SIDE, pCb | (pSb << 1));
+        fl = (fl & ~(15u << W_VC) & ~W_STARTS & ~W_PXNE) | ((uint32_t)vclass << W_VC);
+        if (contributing && (vclass == LED || vclass == RED) && R.by == yb) fl |= W_STARTS;
+      }
+      const bool handled = contributing && vclass != NUL && vclass != TED && vclass != BED && vclass != FUL;
+      const unsigned lh = __ballot_sync(kFull, handled) & lt;
+      const double xbs = valid ? R.xb : 0.0;
+      const double pxl = __shfl_sync(kFull, xbs, lh ? 31 - __clz(lh) : lane);
+      const double px_before = lh ? pxl : -kDblMax;
+      const bool copy = contributing && (vclass == LED || vclass == RED) && !(fl & W_STARTS);
+      if (exists) {
+        if (xbs != px_before) fl |= W_PXNE;
+        R.fl = fl;
+        if (copy) R.outA = R.outB;
+      }
+      mc = __ballot_sync(kFull, contributing && !copy);
+      any_fix = __any_sync(kFull, valid && R.ty == yb && fbits(fl, W_STB) == BUNDLE_HEAD);
+    }
+
+    // ---- output, in AET order: lane 0 runs the events, the warp the redirects
+    if (mc) {
+      for (unsigned m = mc; m; m &= m - 1) {
+        const int s = __ffs(m) - 1;
+        const uint32_t fl = __shfl_sync(kFull, R.fl, s);
+        const double xb = __shfl_sync(kFull, R.xb, s);
+        int oa = __shfl_sync(kFull, R.outA, s), ob = __shfl_sync(kFull, R.outB, s);
+        int rt = -1, rto = -1;
+        if (lane == 0 && !A.status) wout_event(A, P, fl, xb, yb, oa, ob, cf, out_poly, rt, rto);
+        oa = __shfl_sync(kFull, oa, 0);
+        ob = __shfl_sync(kFull, ob, 0);
+        if (lane == s) {
+          R.outA = oa;
+          R.outB = ob;
+        }
+        rt = __shfl_sync(kFull, rt, 0);
+        if (rt >= 0) wp_redirect_all(P, __shfl_sync(kFull, A.np, 0), rt, __shfl_sync(kFull, rto, 0));
+      }
+      __syncwarp();
+      A.status = __shfl_sync(kFull, A.status, 0);
+      out_poly = __shfl_sync(kFull, out_poly, 0);
+      if (A.status) {
+        ret = kBeamsFail;
+        break;
+      }
+    }
+
+    // ---- next scanbeam, delete edges ending at yb, compute xt
+    if (any_fix) {
+      if (valid) wstore(W, lane, R);
+      __syncwarp();
+      if (lane == 0) wfixups(W, n, yb);
+      __syncwarp();
+      if (valid) R = wload(W, lane);
+    }
+    double ny = lmin < A.nb ? bys(lmin) : kInf;
+    {
+      double m = valid && R.ty != yb ? R.ty : kInf;
+      for (int o = 16; o; o >>= 1) {
+        const double t = __shfl_xor_sync(kFull, m, o);
+        m = t < m ? t : m;
+      }
+      ny = m < ny ? m : ny;
+    }
+    if (!(ny < kInf)) break;  // the last beam
+    yt = ny;
+    dy = yt - yb;
+    {
+      const bool keep = valid && R.ty != yb;
+      const unsigned km = __ballot_sync(kFull, keep), vm = __ballot_sync(kFull, valid);
+      if (keep) R.xt = R.ty == yt ? R.tx : R.bx + R.dx * (yt - R.by);
+      if (km != vm) R = wshfl(R, lane < __popc(km) ? nth_bit(km, lane) : lane);
+      n = __popc(km);
+    }
+
+    // ---- intersections
+    {
+      const bool v2 = lane < n;
+      const bool el = v2 && (fbits(R.fl, W_STA) == BUNDLE_HEAD || fbits(R.fl, W_BA) != 0);
+      const unsigned lower = __ballot_sync(kFull, el) & lt;
+      const int pj = lower ? 31 - __clz(lower) : lane;
+      const double qxb = __shfl_sync(kFull, R.xb, pj), qxt = __shfl_sync(kFull, R.xt, pj),
+                   qdx = __shfl_sync(kFull, R.dx, pj);
+      bool good = true;
+      if (el && lower) {
+        const double den = (qxt - qxb) - (R.xt - R.xb);
+        good = R.xt >= qxt || R.dx == qdx || fabs(den) <= kEps;
+      }
+      if (!__all_sync(kFull, good)) {
+        if (v2) wstore(W, lane, R);
+        __syncwarp();
+        if (wintersect(A, W, P, op, n, yb, dy, out_poly, mode)) {
+          ret = kBeamsFail;
+          break;
+        }
+        if (v2) R = wload(W, lane);
+      }
+    }
+
+    // ---- successors of edges ending at yt; state below := state above
+    if (lane < n) {
+      const int oa = R.outA, sta = fbits(R.fl, W_STA), ba = fbits(R.fl, W_BA);
+      const int sc = R.ty == yt ? R.succ : -1;
+      if (sc >= 0) {
+        WSlot v = wslot_of(A, sc);
+        v.outB = oa;
+        v.fl = fset(fset(v.fl, W_STB, sta), W_BB, ba);
+        v.outA = -1;
+        R = v;
+      } else {
+        R.outB = oa;
+        R.fl = fset(fset(R.fl, W_STB, sta), W_BB, ba);
+        R.xb = R.xt;
+        R.outA = -1;
+      }
+    }
+    yb = yt;
+  }
+  S.yb = yb;
+  S.yt = yt;
+  S.dy = dy;
+  S.bwin = bwin;
+  S.n = n;
+  S.lmin = lmin;
+  S.cf = cf;
+  S.out_poly = out_poly;
+  S.bbase = bbase;
+  return ret;
+}
+
 template <int op>
 __device__ __noinline__ int wclip_impl(Arena &A, const PolyView &subj, const PolyView &clip, WAet &W, int *mode) {
   const int lane = threadIdx.x & 31;
@@ -614,7 +1082,24 @@ __device__ __noinline__ int wclip_impl(Arena &A, const PolyView &subj, const Pol
     return __shfl_sync(kFull, bwin, i - bbase);
   };
   double yb = bys(0);  // the lowest vertex is a local minimum
+  bool grown = false;  // this beam's insertion outgrew the register loop
   for (;;) {
+    if (n <= 32 && !grown) {
+      WBeams S{yb, yt, dy, bwin, n, lmin, cf, out_poly, bbase};
+      const int r = wbeams_reg<op>(A, W, P, S, mode);
+      yb = S.yb;
+      yt = S.yt;
+      dy = S.dy;
+      bwin = S.bwin;
+      n = S.n;
+      lmin = S.lmin;
+      cf = S.cf;
+      out_poly = S.out_poly;
+      bbase = S.bbase;
+      if (r == kBeamsDone) break;
+      if (r == kBeamsFail) return -1;
+      grown = true;  // kBeamsGrow: the insertion goes on below
+    }
     // ---- local minima at yb into the AET (add_edge_to_aet)
     while (lmin < A.nb && bys(lmin) == yb) {
       const int e = A.B[lmin++].edge;
@@ -842,81 +1327,7 @@ __device__ __noinline__ int wclip_impl(Arena &A, const PolyView &subj, const Pol
           const int s = c + __ffs(m) - 1;
           m &= m - 1;
           int rt = -1, rto = -1;
-          if (lane == 0 && !A.status) {
-            const uint32_t fl = W.fl()[s];
-            const int vclass = (int)((fl >> W_VC) & 15u);
-            const double xb = W.xb()[s];
-            const bool pxne = (fl & W_PXNE) != 0;
-            int &oa = W.outA()[s];
-            int &ob = W.outB()[s];
-            switch (vclass) {
-              case EMN:
-              case IMN: {
-                const int k = wp_local_min(A, P, out_poly, xb, yb);
-                if (k >= 0) oa = k;
-                cf = oa;
-                break;
-              }
-              case ERI:
-                if (pxne) wp_add_right(A, P, cf, xb, yb);
-                oa = cf;
-                cf = -1;
-                break;
-              case ELI:
-                wp_add_left(A, P, ob, xb, yb);
-                cf = ob;
-                break;
-              case EMX:
-                if (pxne) wp_add_left(A, P, cf, xb, yb);
-                rt = wp_merge_right(A, P, cf, ob, &rto);
-                cf = -1;
-                break;
-              case ILI:
-                if (pxne) wp_add_left(A, P, cf, xb, yb);
-                oa = cf;
-                cf = -1;
-                break;
-              case IRI:
-                wp_add_right(A, P, ob, xb, yb);
-                cf = ob;
-                ob = -1;
-                break;
-              case IMX:
-                if (pxne) wp_add_right(A, P, cf, xb, yb);
-                rt = wp_merge_left(A, P, cf, ob, &rto);
-                cf = -1;
-                ob = -1;
-                break;
-              case IMM: {
-                if (pxne) wp_add_right(A, P, cf, xb, yb);
-                rt = wp_merge_left(A, P, cf, ob, &rto);
-                ob = -1;
-                const int k = wp_local_min(A, P, out_poly, xb, yb);
-                if (k >= 0) oa = k;
-                cf = oa;
-                break;
-              }
-              case EMM: {
-                if (pxne) wp_add_left(A, P, cf, xb, yb);
-                rt = wp_merge_right(A, P, cf, ob, &rto);
-                ob = -1;
-                const int k = wp_local_min(A, P, out_poly, xb, yb);
-                if (k >= 0) oa = k;
-                cf = oa;
-                break;
-              }
-              case LED:
-                if (fl & W_STARTS) wp_add_left(A, P, ob, xb, yb);
-                oa = ob;
-                break;
-              case RED:
-                if (fl & W_STARTS) wp_add_right(A, P, ob, xb, yb);
-                oa = ob;
-                break;
-              default:
-                break;
-            }
-          }
+          if (lane == 0 && !A.status) wout_event(A, P, W.fl()[s], W.xb()[s], yb, W.outA()[s], W.outB()[s], cf, out_poly, rt, rto);
           rt = __shfl_sync(kFull, rt, 0);
           if (rt >= 0) {
             // the new local minimum of IMM / EMM (if any) is past the old list
@@ -936,21 +1347,7 @@ __device__ __noinline__ int wclip_impl(Arena &A, const PolyView &subj, const Pol
     {
       if (any_fix) {
         // bundle fix-ups of deleted bundle heads, in AET order (lane 0)
-        if (lane == 0) {
-          for (int d = 0; d < n; d++) {
-            if (!(W.ty()[d] == yb && fbits(W.fl()[d], W_STB) == BUNDLE_HEAD)) continue;
-            int pe = d - 1;
-            while (pe >= 0 && W.ty()[pe] == yb) pe--;
-            if (pe < 0) continue;
-            if (fbits(W.fl()[pe], W_STB) == BUNDLE_TAIL) {
-              W.outB()[pe] = W.outB()[d];
-              W.fl()[pe] = fset(W.fl()[pe], W_STB, UNBUNDLED);
-              int pp = pe - 1;
-              while (pp >= 0 && W.ty()[pp] == yb) pp--;
-              if (pp >= 0 && fbits(W.fl()[pp], W_STB) == BUNDLE_TAIL) W.fl()[pe] = fset(W.fl()[pe], W_STB, BUNDLE_HEAD);
-            }
-          }
-        }
+        if (lane == 0) wfixups(W, n, yb);
         __syncwarp();
       }
       // the next scanbeam y: the lowest top of the edges that go on, or the
@@ -1045,46 +1442,7 @@ __device__ __noinline__ int wclip_impl(Arena &A, const PolyView &subj, const Pol
           hdx = __shfl_sync(kFull, dx, lj);
         }
       }
-      if (!ok) {
-        // spill to the linked form, run the thread clipper's step, reload
-        for (int c = 0; c < n; c += 32) {
-          const int s = c + lane;
-          if (s < n) wspill(A, wload(W, s), s > 0 ? W.edge()[s - 1] : -1, s + 1 < n ? W.edge()[s + 1] : -1);
-        }
-        __syncwarp();
-        wp_sync(P, A.np, 0);
-        int bad = 0;
-        if (lane == 0) {
-          int aet = W.edge()[0];
-          intersect_beam(A, op, aet, out_poly, yb, dy);
-          if (!A.status) {
-            int cur = aet, k = 0;
-            while (cur >= 0 && k < n) {
-              W.ord()[k++] = cur;
-              cur = A.E[cur].next;
-            }
-            bad = (k != n || cur >= 0) ? 1 : 0;
-          }
-        }
-        __syncwarp();
-        A.status = __shfl_sync(kFull, A.status, 0);
-        out_poly = __shfl_sync(kFull, out_poly, 0);
-        bad = __shfl_sync(kFull, bad, 0);
-        wp_sync(P, A.np, 1);
-        if (bad) {
-          *mode = kWarpFallback;
-          return -1;
-        }
-        if (A.status) return -1;
-        for (int c = 0; c < n; c += 32) {
-          const int s = c + lane;
-          WSlot v;
-          if (s < n) v = wslot_of(A, W.ord()[s]);
-          __syncwarp();
-          if (s < n) wstore(W, s, v);
-        }
-        __syncwarp();
-      }
+      if (!ok && wintersect(A, W, P, op, n, yb, dy, out_poly, mode)) return -1;
     }
 
     // ---- successors of edges ending at yt; state below := state above (GPC:661-693)
@@ -1110,6 +1468,7 @@ __device__ __noinline__ int wclip_impl(Arena &A, const PolyView &subj, const Pol
     }
     __syncwarp();
     yb = yt;
+    grown = false;
   }
   wp_sync(P, A.np, 0);  // the result readers use the arena's nodes
   return out_poly;
