@@ -252,9 +252,10 @@ int prt_clip_pair_host(int op, int s_ncont, const int32_t *s_nverts, const doubl
  * pairs whose vertex count n_subject + n_clip lies in
  * (bin_thresholds[b+1], bin_thresholds[b]]; bins are clipped largest first
  * in one persistent launch.  bin_warp_mode[b] = 1 clips each pair of the bin
- * with a whole warp (active edge table in shared memory, aet_slots slots per
- * warp, a larger table moves to the pair's arena), 0 with one
- * thread per pair.  The launch starts warps_per_sm persistent warps per SM;
+ * with a whole warp (an active edge table of up to 32 edges in registers, a
+ * larger one in shared memory, aet_slots slots per warp, a larger one still
+ * in the pair's arena), 0 with one thread per pair.  The launch starts
+ * warps_per_sm persistent warps per SM (at most 12, the resident limit);
  * every warp takes the next pair (warp mode) or the next 32 pairs (thread
  * mode) of the largest bin that still has pairs, so the largest pairs are
  * clipped first by all warps. */

@@ -295,9 +295,9 @@ class _Schedule(C.Structure):
         s = cls()
         thr = list(d["thresholds"])
         s.nbins = len(thr)
-        s.aet_slots = int(d.get("aet_slots", 128))
+        s.aet_slots = int(d.get("aet_slots", 64))
         wm = list(d.get("warp_mode", [1] * len(thr)))
-        s.warps_per_sm = int(d.get("warps_per_sm", 8))
+        s.warps_per_sm = int(d.get("warps_per_sm", 12))
         for b in range(len(thr)):
             s.bin_thresholds[b] = int(thr[b])
             s.bin_warp_mode[b] = int(wm[b])

@@ -168,7 +168,7 @@ int prt_autotune(const prt_layer *base, const prt_layer *overlay, int op, int64_
     return PRT_OK;
   };
   int64_t warp_above = 256;
-  int slots = 128, wps = 8;
+  int slots = 64, wps = kLptWarpsPerSM;
   prt_schedule best = make_schedule(warp_above, slots, wps);
   double best_ms = 1e30;
   if (!rc && m > 0) {
@@ -185,7 +185,7 @@ int prt_autotune(const prt_layer *base, const prt_layer *overlay, int op, int64_
         warp_above = wa;
       }
     }
-    const int cands_s[] = {64, 256};
+    const int cands_s[] = {32, 128};
     for (int sl : cands_s) {
       if (rc || secs_since(t0) > time_budget_s) break;
       prt_schedule c = make_schedule(warp_above, sl, wps);
@@ -197,7 +197,7 @@ int prt_autotune(const prt_layer *base, const prt_layer *overlay, int op, int64_
         slots = sl;
       }
     }
-    const int cands_wp[] = {4, 6, 12, 16};
+    const int cands_wp[] = {4, 6, 8, 10};
     for (int wp : cands_wp) {
       if (rc || secs_since(t0) > time_budget_s) break;
       prt_schedule c = make_schedule(warp_above, slots, wp);

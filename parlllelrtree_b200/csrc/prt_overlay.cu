@@ -181,10 +181,13 @@ __global__ void __launch_bounds__(128) clip_plain_kernel(PairSrc S, ClipOut O, c
 // 32 in thread mode), then steals from the smaller bins after it.  One warp
 // per block spreads the big-pair warps over every SM; the block's dynamic
 // shared memory holds the warp clipper's active-edge slots.
-__global__ void __launch_bounds__(32, 8) clip_lpt_kernel(PairSrc S, ClipOut O, const uint32_t *__restrict__ order,
-                                                         BinPlan plan, unsigned long long *tickets,
-                                                         unsigned char *arena, int scale,
-                                                         const int64_t *__restrict__ dyn_ranges) {
+// Compiled for kLptWarpsPerSM resident warps per SM (at most 168 registers a
+// thread): with fewer, the warp clipper's shuffle and FP64 latencies go
+// unhidden; with more, its register loop spills.
+__global__ void __launch_bounds__(32, kLptWarpsPerSM)
+    clip_lpt_kernel(PairSrc S, ClipOut O, const uint32_t *__restrict__ order, BinPlan plan,
+                    unsigned long long *tickets, unsigned char *arena, int scale,
+                    const int64_t *__restrict__ dyn_ranges) {
   __shared__ int64_t s_begin[PRT_MAX_BINS], s_end[PRT_MAX_BINS];
   __shared__ int32_t s_mode[PRT_MAX_BINS];
   const int lane = threadIdx.x & 31;
@@ -328,14 +331,15 @@ size_t arena_budget() {
 
 // ---- batched schedule ----------------------------------------------------------
 // Default: pairs above 256 vertices are clipped one per warp, smaller ones one
-// per thread; 8 warps per SM, what an SM holds at the clip kernel's register
-// count.
+// per thread; kLptWarpsPerSM warps per SM, what an SM holds at the clip
+// kernel's register count; 64 shared-memory slots per warp (the warp
+// clipper keeps active edge tables of up to 32 edges in registers).
 static prt_schedule default_schedule() {
   prt_schedule d;
   memset(&d, 0, sizeof d);
   d.nbins = 5;
-  d.aet_slots = 128;
-  d.warps_per_sm = 8;
+  d.aet_slots = 64;
+  d.warps_per_sm = kLptWarpsPerSM;
   const int64_t thr[5] = {1ll << 40, 4096, 1024, 256, 64};
   const int32_t wm[5] = {1, 1, 1, 0, 0};
   for (int b = 0; b < 5; b++) {
@@ -392,7 +396,8 @@ size_t plan_bins(const prt_schedule &sc, const int64_t *counts, const int64_t *m
     work += sc.bin_warp_mode[b] ? counts[b] : (counts[b] + 31) / 32;
   }
   region = (region + 511) & ~(int64_t)511;
-  int64_t warps = std::min<int64_t>(work, (int64_t)kSMs * sc.warps_per_sm);
+  // no more warps than can be resident: the persistent launch must not queue
+  int64_t warps = std::min<int64_t>(work, (int64_t)kSMs * std::min(sc.warps_per_sm, kLptWarpsPerSM));
   warps = std::min<int64_t>(warps, (int64_t)(budget / (size_t)region));
   if (work > 0) warps = std::max<int64_t>(warps, 1);
   for (int b = 0; b <= sc.nbins; b++) plan.warp0[b] = b == 0 ? 0 : warps;

@@ -46,6 +46,10 @@ int overlay_impl(const PairSrc &S, int64_t n, int sched, double *d_area, cudaStr
 
 namespace prt {
 
+// Resident warps per SM of the persistent batched clip launch (its launch
+// bounds); a schedule's warps_per_sm is capped at it.
+constexpr int kLptWarpsPerSM = 12;
+
 // Bins of the batched schedule, size-descending: bin b holds sorted positions
 // [begin[b], end[b]).  Warps [warp0[g], warp0[g+1]) start on bin g with
 // region[g] bytes of arena each (one pair of any later bin in warp mode, or

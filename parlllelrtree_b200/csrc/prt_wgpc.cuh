@@ -801,12 +801,35 @@ __device__ __noinline__ int wbeams_reg(Arena &A, const WAet &W, const WPoly &P, 
   const int lane = threadIdx.x & 31;
   const unsigned lt = lanemask_lt();
   const int pC0 = op == OP_DIFF ? RIGHT : LEFT;
+  // the initial sides of every edge (bside[CLIP], bside[SUBJ])
+  constexpr uint32_t kSides = (uint32_t)((op == OP_DIFF ? RIGHT : LEFT) | (LEFT << 1)) << W_SIDE;
   int n = S.n, lmin = S.lmin, cf = S.cf, out_poly = S.out_poly, bbase = S.bbase;
-  double yb = S.yb, yt = S.yt, dy = S.dy, bwin = S.bwin;
+  double yb = S.yb, yt = S.yt, dy = S.dy;
+  // local-minima window: bound bbase + lane and the static fields of its
+  // first edge, read 32 at a time
+  double bwin = 0.0, wx = 0.0, wdx = 0.0, wtx = 0.0, wty = 0.0;
+  int wedge = -1, wsucc = -1, wtype = 0;
+  auto load_win = [&]() {
+    const int k = bbase + lane;
+    bwin = 0.0;
+    if (k < A.nb) {
+      const Bound &b = A.B[k];
+      bwin = b.y;
+      wx = b.x;
+      wdx = b.dx;
+      wedge = b.edge;
+      const Edge &E = A.E[wedge];
+      wtx = E.tx;
+      wty = E.ty;
+      wsucc = E.succ;
+      wtype = E.type;
+    }
+  };
+  load_win();
   auto bys = [&](int i) -> double {
     if (i - bbase >= 32) {
       bbase += 32 * ((i - bbase) / 32);
-      bwin = bbase + lane < A.nb ? A.B[bbase + lane].y : 0.0;
+      load_win();
     }
     return __shfl_sync(kFull, bwin, i - bbase);
   };
@@ -821,7 +844,22 @@ __device__ __noinline__ int wbeams_reg(Arena &A, const WAet &W, const WPoly &P, 
         grow = true;
         break;
       }
-      const WSlot ns = wslot_of(A, A.B[lmin++].edge);
+      // the bound's first edge as wslot_of would read it: an edge that has
+      // not been active keeps the build's values (xb = bx = the bound's x,
+      // by = its y, the bound's dx, xt = 0, no output polygons or bundles,
+      // the initial sides)
+      const int sl = lmin++ - bbase;
+      WSlot ns;
+      ns.edge = __shfl_sync(kFull, wedge, sl);
+      ns.xb = ns.bx = __shfl_sync(kFull, wx, sl);
+      ns.by = __shfl_sync(kFull, bwin, sl);
+      ns.dx = __shfl_sync(kFull, wdx, sl);
+      ns.tx = __shfl_sync(kFull, wtx, sl);
+      ns.ty = __shfl_sync(kFull, wty, sl);
+      ns.succ = __shfl_sync(kFull, wsucc, sl);
+      ns.xt = 0.0;
+      ns.outA = ns.outB = -1;
+      ns.fl = (__shfl_sync(kFull, wtype, sl) ? W_TYPE : 0u) | kSides;
       const unsigned m = __ballot_sync(kFull, lane < n && (ns.xb < R.xb || (ns.xb == R.xb && ns.dx < R.dx)));
       const int pos = m ? __ffs(m) - 1 : n;
       const WSlot up = wshfl_up(R);
@@ -1044,7 +1082,7 @@ __device__ __noinline__ int wbeams_reg(Arena &A, const WAet &W, const WPoly &P, 
   S.yb = yb;
   S.yt = yt;
   S.dy = dy;
-  S.bwin = bwin;
+  S.bwin = bwin;  // bound bbase + lane's y: the shared-memory loop's window
   S.n = n;
   S.lmin = lmin;
   S.cf = cf;
