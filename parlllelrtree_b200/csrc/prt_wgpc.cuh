@@ -442,8 +442,29 @@ __device__ inline bool wbuild(Arena &A, int op, const PolyView &subj, const Poly
     }
   }
   if (A.status || A.nb == 0) return true;
-  // local-minima table: (y, x, dx), ties in creation order = three stable
-  // passes, least significant key first
+  // local-minima table: (y, x, dx), ties in creation order
+  if (A.nb <= 32) {
+    // one bound per lane, placed at its rank
+    const bool v = lane < A.nb;
+    Bound b;
+    uint64_t ky = 0, kx = 0, kd = 0;
+    if (v) {
+      b = A.B[lane];
+      ky = dkey(b.y);
+      kx = dkey(b.x);
+      kd = dkey(b.dx);
+    }
+    int rank = 0;
+    for (int k = 0; k < A.nb; k++) {
+      const uint64_t oy = __shfl_sync(kFull, ky, k), ox = __shfl_sync(kFull, kx, k), od = __shfl_sync(kFull, kd, k);
+      rank += oy < ky || (oy == ky && (ox < kx || (ox == kx && (od < kd || (od == kd && k < lane)))));
+    }
+    __syncwarp();
+    if (v) A.B[rank] = b;
+    __syncwarp();
+    return true;
+  }
+  // more: three stable radix sorts, least significant key first
   uint32_t *cnt = wsm_counters(W.scap);
   Bound *bs = reinterpret_cast<Bound *>(A.IT);
   Bound *cur = warp_radix(A.B, bs, A.nb, [](const Bound &b) { return dkey(b.dx); }, cnt);
@@ -762,6 +783,111 @@ __device__ inline WSlot wshfl_up(const WSlot &v) {
   return r;
 }
 
+// GPC's output at one crossing of two contributing edges (GPC:487-619), on
+// one lane: f0 / f1 are the flags of the left and right edge, o0 / o1 their
+// output polygons above (updated).  A contour merge returns in rt the proxy
+// to redirect and in rto its replacement.
+template <int op>
+__device__ inline void wcross_event(Arena &A, const WPoly &P, uint32_t f0, uint32_t f1, double ix, double iy, int &o0,
+                                    int &o1, int &out_poly, int &rt, int &rto) {
+  const int ba0 = fbits(f0, W_BA), ba1 = fbits(f1, W_BA), s0 = fbits(f0, W_SIDE), s1 = fbits(f1, W_SIDE);
+  const int b0C = ba0 & 1, b0S = ba0 >> 1, b1C = ba1 & 1, b1S = ba1 >> 1;
+  const int s0C = s0 & 1, s0S = s0 >> 1, s1C = s1 & 1, s1S = s1 >> 1;
+  const int inC = (b0C && !s0C) || (b1C && s1C) || (!b0C && !b1C && s0C && s1C);
+  const int inS = (b0S && !s0S) || (b1S && s1S) || (!b0S && !b1S && s0S && s1S);
+  int tr, tl, br, bl;
+  if (op == OP_DIFF || op == OP_INT) {
+    tr = inC && inS;
+    tl = (inC ^ b1C) && (inS ^ b1S);
+    br = (inC ^ b0C) && (inS ^ b0S);
+    bl = (inC ^ b1C ^ b0C) && (inS ^ b1S ^ b0S);
+  } else if (op == OP_XOR) {
+    tr = inC ^ inS;
+    tl = (inC ^ b1C) ^ (inS ^ b1S);
+    br = (inC ^ b0C) ^ (inS ^ b0S);
+    bl = (inC ^ b1C ^ b0C) ^ (inS ^ b1S ^ b0S);
+  } else {
+    tr = inC || inS;
+    tl = (inC ^ b1C) || (inS ^ b1S);
+    br = (inC ^ b0C) || (inS ^ b0S);
+    bl = (inC ^ b1C ^ b0C) || (inS ^ b1S ^ b0S);
+  }
+  const int p = o0, q = o1;
+  switch (tr + (tl << 1) + (br << 2) + (bl << 3)) {
+    case EMN:
+    case IMN: {
+      const int k = wp_local_min(A, P, out_poly, ix, iy);
+      if (k >= 0) o0 = k;
+      o1 = o0;
+      break;
+    }
+    case ERI:
+      if (p >= 0) {
+        wp_add_right(A, P, p, ix, iy);
+        o1 = p;
+        o0 = -1;
+      }
+      break;
+    case ELI:
+      if (q >= 0) {
+        wp_add_left(A, P, q, ix, iy);
+        o0 = q;
+        o1 = -1;
+      }
+      break;
+    case EMX:
+      if (p >= 0 && q >= 0) {
+        wp_add_left(A, P, p, ix, iy);
+        rt = wp_merge_right(A, P, p, q, &rto);
+        o0 = -1;
+        o1 = -1;
+      }
+      break;
+    case ILI:
+      if (p >= 0) {
+        wp_add_left(A, P, p, ix, iy);
+        o1 = p;
+        o0 = -1;
+      }
+      break;
+    case IRI:
+      if (q >= 0) {
+        wp_add_right(A, P, q, ix, iy);
+        o0 = q;
+        o1 = -1;
+      }
+      break;
+    case IMX:
+      if (p >= 0 && q >= 0) {
+        wp_add_right(A, P, p, ix, iy);
+        rt = wp_merge_left(A, P, p, q, &rto);
+        o0 = -1;
+        o1 = -1;
+      }
+      break;
+    case IMM:
+      if (p >= 0 && q >= 0) {
+        wp_add_right(A, P, p, ix, iy);
+        rt = wp_merge_left(A, P, p, q, &rto);
+        const int k = wp_local_min(A, P, out_poly, ix, iy);
+        if (k >= 0) o0 = k;
+        o1 = o0;
+      }
+      break;
+    case EMM:
+      if (p >= 0 && q >= 0) {
+        wp_add_left(A, P, p, ix, iy);
+        rt = wp_merge_right(A, P, p, q, &rto);
+        const int k = wp_local_min(A, P, out_poly, ix, iy);
+        if (k >= 0) o0 = k;
+        o1 = o0;
+      }
+      break;
+    default:
+      break;
+  }
+}
+
 // Position of the k-th (0-based) set bit of m; m has more than k set bits.
 __device__ inline int nth_bit(unsigned m, int k) {
   int pos = 0;
@@ -1050,13 +1176,89 @@ __device__ __noinline__ int wbeams_reg(Arena &A, const WAet &W, const WPoly &P, 
         good = R.xt >= qxt || R.dx == qdx || fabs(den) <= kEps;
       }
       if (!__all_sync(kFull, good)) {
-        if (v2) wstore(W, lane, R);
-        __syncwarp();
-        if (wintersect(A, W, P, op, n, yb, dy, out_poly, mode)) {
-          ret = kBeamsFail;
-          break;
+        // the intersection table (build_intersection_table, GPC:1309-1471):
+        // eligible slots enter the sorted edge table (ST) in AET order; an
+        // entering edge walks the ST from its head and records a crossing
+        // with every member it passes, up to the first member it stops at.
+        // ST positions live in the lanes (0 = head), the stop is found with
+        // one OR-reduction per entering edge.
+        int pos = -1, k = 0, nrec = 0, l0 = -1, l1 = -1;
+        double ixr = 0.0, iyr = 0.0;  // the first crossing, on the lane of its ST member
+        for (unsigned todo = __ballot_sync(kFull, el); todo; todo &= todo - 1) {
+          const int le = __ffs(todo) - 1;
+          const double exb = __shfl_sync(kFull, R.xb, le), ext = __shfl_sync(kFull, R.xt, le),
+                       edx = __shfl_sync(kFull, R.dx, le);
+          double den = 0.0;
+          bool stop = false;
+          if (pos >= 0) {
+            den = (R.xt - R.xb) - (ext - exb);
+            stop = ext >= R.xt || edx == R.dx || fabs(den) <= kEps;
+          }
+          const unsigned sm = __reduce_or_sync(kFull, pos >= 0 && stop ? 1u << pos : 0u);
+          const int q = sm ? __ffs(sm) - 1 : k;
+          if (q > 0 && nrec == 0) {
+            l0 = __ffs(__ballot_sync(kFull, pos == 0)) - 1;
+            l1 = le;
+            if (lane == l0) {
+              const double rr = (exb - R.xb) / den;
+              ixr = R.xb + rr * (R.xt - R.xb);
+              iyr = rr * dy;
+            }
+          }
+          nrec += q;
+          if (nrec > 1) break;
+          if (pos >= q) pos++;
+          if (lane == le) pos = q;
+          k++;
         }
-        if (v2) R = wload(W, lane);
+        if (nrec == 1) {
+          // one crossing, of slots l0 < l1 (GPC:487-657 for one table entry)
+          const uint32_t f0 = __shfl_sync(kFull, R.fl, l0), f1 = __shfl_sync(kFull, R.fl, l1);
+          int o0 = __shfl_sync(kFull, R.outA, l0), o1 = __shfl_sync(kFull, R.outA, l1);
+          const double ix = __shfl_sync(kFull, ixr, l0), iy = __shfl_sync(kFull, iyr, l0) + yb;
+          const int ba0 = fbits(f0, W_BA), ba1 = fbits(f1, W_BA);
+          int rt = -1, rto = -1;
+          if (ba0 && ba1 && lane == 0 && !A.status) wcross_event<op>(A, P, f0, f1, ix, iy, o0, o1, out_poly, rt, rto);
+          o0 = __shfl_sync(kFull, o0, 0);
+          o1 = __shfl_sync(kFull, o1, 0);
+          rt = __shfl_sync(kFull, rt, 0);
+          if (rt >= 0) wp_redirect_all(P, __shfl_sync(kFull, A.np, 0), rt, __shfl_sync(kFull, rto, 0));
+          A.status = __shfl_sync(kFull, A.status, 0);
+          out_poly = __shfl_sync(kFull, out_poly, 0);
+          if (A.status) {
+            ret = kBeamsFail;
+            break;
+          }
+          // outputs above, sides flipped by the other edge's bundle
+          if (lane == l0) {
+            R.outA = o0;
+            R.fl ^= (uint32_t)ba1 << W_SIDE;
+          }
+          if (lane == l1) {
+            R.outA = o1;
+            R.fl ^= (uint32_t)ba0 << W_SIDE;
+          }
+          // swap the bundle of l0 (with the tails before it) and the slots up
+          // to l1: GPC steps over l0's predecessor, then over bundle tails
+          int b0 = l0;
+          if (fbits(f0, W_STA) == BUNDLE_HEAD) {
+            const unsigned tails = __ballot_sync(kFull, v2 && fbits(R.fl, W_STA) == BUNDLE_TAIL);
+            const unsigned others = ~tails & (l0 >= 1 ? (1u << (l0 - 1)) - 1u : 0u);
+            b0 = others ? 32 - __clz(others) : 0;
+          }
+          const int len2 = l1 - l0;
+          int src = lane;
+          if (lane >= b0 && lane <= l1) src = lane < b0 + len2 ? l0 + 1 + (lane - b0) : b0 + (lane - b0 - len2);
+          R = wshfl(R, src);
+        } else {
+          if (v2) wstore(W, lane, R);
+          __syncwarp();
+          if (wintersect(A, W, P, op, n, yb, dy, out_poly, mode)) {
+            ret = kBeamsFail;
+            break;
+          }
+          if (v2) R = wload(W, lane);
+        }
       }
     }
 
