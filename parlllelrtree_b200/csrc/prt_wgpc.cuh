@@ -783,6 +783,23 @@ __device__ inline WSlot wshfl_up(const WSlot &v) {
   return r;
 }
 
+// Source lane of each slot after GPC's swap of two crossing bundles
+// (GPC:622-657): the bundle of slot l0 (with the tail slots before it, when
+// l0 is a bundle head; GPC steps over l0's predecessor, then over tails) moves
+// to just after slot l1, and the slots between move down.  tails: the lanes
+// whose edges are bundle tails; sta0: slot l0's bundle state.
+__device__ inline int wswap_src(unsigned tails, int sta0, int l0, int l1) {
+  const int lane = threadIdx.x & 31;
+  int b0 = l0;
+  if (sta0 == BUNDLE_HEAD) {
+    const unsigned others = ~tails & (l0 >= 1 ? (1u << (l0 - 1)) - 1u : 0u);
+    b0 = others ? 32 - __clz(others) : 0;
+  }
+  const int len2 = l1 - l0;
+  if (lane < b0 || lane > l1) return lane;
+  return lane < b0 + len2 ? l0 + 1 + (lane - b0) : b0 + (lane - b0 - len2);
+}
+
 // GPC's output at one crossing of two contributing edges (GPC:487-619), on
 // one lane: f0 / f1 are the flags of the left and right edge, o0 / o1 their
 // output polygons above (updated).  A contour merge returns in rt the proxy
@@ -1181,13 +1198,16 @@ __device__ __noinline__ int wbeams_reg(Arena &A, const WAet &W, const WPoly &P, 
         // entering edge walks the ST from its head and records a crossing
         // with every member it passes, up to the first member it stops at.
         // ST positions live in the lanes (0 = head), the stop is found with
-        // one OR-reduction per entering edge.
-        int pos = -1, k = 0, nrec = 0, l0 = -1, l1 = -1;
-        double ixr = 0.0, iyr = 0.0;  // the first crossing, on the lane of its ST member
+        // one OR-reduction per entering edge.  Crossing i (in recording
+        // order) goes to entry i of the slot arrays W, unused in this loop:
+        // x in xb, the beam-relative y in xt, the two edges in edge / outA.
+        int pos = -1, k = 0, nrec = 0;
+        bool many = false;  // more than 32 crossings
         for (unsigned todo = __ballot_sync(kFull, el); todo; todo &= todo - 1) {
           const int le = __ffs(todo) - 1;
           const double exb = __shfl_sync(kFull, R.xb, le), ext = __shfl_sync(kFull, R.xt, le),
                        edx = __shfl_sync(kFull, R.dx, le);
+          const int eid = __shfl_sync(kFull, R.edge, le);
           double den = 0.0;
           bool stop = false;
           if (pos >= 0) {
@@ -1196,60 +1216,96 @@ __device__ __noinline__ int wbeams_reg(Arena &A, const WAet &W, const WPoly &P, 
           }
           const unsigned sm = __reduce_or_sync(kFull, pos >= 0 && stop ? 1u << pos : 0u);
           const int q = sm ? __ffs(sm) - 1 : k;
-          if (q > 0 && nrec == 0) {
-            l0 = __ffs(__ballot_sync(kFull, pos == 0)) - 1;
-            l1 = le;
-            if (lane == l0) {
-              const double rr = (exb - R.xb) / den;
-              ixr = R.xb + rr * (R.xt - R.xb);
-              iyr = rr * dy;
-            }
+          if (nrec + q > 32) {
+            many = true;
+            break;
+          }
+          if (pos >= 0 && pos < q) {
+            const double rr = (exb - R.xb) / den;
+            const int i = nrec + pos;
+            W.xb()[i] = R.xb + rr * (R.xt - R.xb);
+            W.xt()[i] = rr * dy;
+            W.edge()[i] = R.edge;
+            W.outA()[i] = eid;
           }
           nrec += q;
-          if (nrec > 1) break;
           if (pos >= q) pos++;
           if (lane == le) pos = q;
           k++;
         }
-        if (nrec == 1) {
-          // one crossing, of slots l0 < l1 (GPC:487-657 for one table entry)
-          const uint32_t f0 = __shfl_sync(kFull, R.fl, l0), f1 = __shfl_sync(kFull, R.fl, l1);
-          int o0 = __shfl_sync(kFull, R.outA, l0), o1 = __shfl_sync(kFull, R.outA, l1);
-          const double ix = __shfl_sync(kFull, ixr, l0), iy = __shfl_sync(kFull, iyr, l0) + yb;
-          const int ba0 = fbits(f0, W_BA), ba1 = fbits(f1, W_BA);
-          int rt = -1, rto = -1;
-          if (ba0 && ba1 && lane == 0 && !A.status) wcross_event<op>(A, P, f0, f1, ix, iy, o0, o1, out_poly, rt, rto);
-          o0 = __shfl_sync(kFull, o0, 0);
-          o1 = __shfl_sync(kFull, o1, 0);
-          rt = __shfl_sync(kFull, rt, 0);
-          if (rt >= 0) wp_redirect_all(P, __shfl_sync(kFull, A.np, 0), rt, __shfl_sync(kFull, rto, 0));
-          A.status = __shfl_sync(kFull, A.status, 0);
-          out_poly = __shfl_sync(kFull, out_poly, 0);
-          if (A.status) {
+        __syncwarp();
+        // the table in y order, ties in recording order (add_intersection):
+        // crossing `lane` has rank `rk`
+        bool regular = !many;
+        double cy = 0.0;
+        int c0 = -1, c1 = -1, rk = 0;
+        if (regular) {
+          if (lane < nrec) {
+            cy = W.xt()[lane];
+            c0 = W.edge()[lane];
+            c1 = W.outA()[lane];
+          }
+          for (int j = 0; j < nrec; j++) {
+            const double oy = __shfl_sync(kFull, cy, j);
+            rk += oy < cy || (oy == cy && j < lane);
+          }
+          // dry run on the edge ids and bundle states: each crossing's left
+          // edge must still be left of its right edge when its turn comes
+          int eid = lane < n ? R.edge : -1, sta = lane < n ? fbits(R.fl, W_STA) : 0;
+          for (int r = 0; r < nrec && regular; r++) {
+            const int cl = __ffs(__ballot_sync(kFull, lane < nrec && rk == r)) - 1;
+            const int e0 = __shfl_sync(kFull, c0, cl), e1 = __shfl_sync(kFull, c1, cl);
+            const int l0 = __ffs(__ballot_sync(kFull, eid == e0)) - 1, l1 = __ffs(__ballot_sync(kFull, eid == e1)) - 1;
+            if (l0 < 0 || l1 <= l0) {
+              regular = false;
+              break;
+            }
+            const int src = wswap_src(__ballot_sync(kFull, sta == BUNDLE_TAIL), __shfl_sync(kFull, sta, l0), l0, l1);
+            eid = __shfl_sync(kFull, eid, src);
+            sta = __shfl_sync(kFull, sta, src);
+          }
+        }
+        if (regular) {
+          // each crossing in turn (GPC:487-657): the output event when both
+          // edges contribute, the side flips, the swap of the two bundles
+          bool failed = false;
+          for (int r = 0; r < nrec; r++) {
+            const int cl = __ffs(__ballot_sync(kFull, lane < nrec && rk == r)) - 1;
+            const int e0 = __shfl_sync(kFull, c0, cl), e1 = __shfl_sync(kFull, c1, cl);
+            const int l0 = __ffs(__ballot_sync(kFull, lane < n && R.edge == e0)) - 1;
+            const int l1 = __ffs(__ballot_sync(kFull, lane < n && R.edge == e1)) - 1;
+            const uint32_t f0 = __shfl_sync(kFull, R.fl, l0), f1 = __shfl_sync(kFull, R.fl, l1);
+            int o0 = __shfl_sync(kFull, R.outA, l0), o1 = __shfl_sync(kFull, R.outA, l1);
+            const double ix = W.xb()[cl], iy = __shfl_sync(kFull, cy, cl) + yb;
+            const int ba0 = fbits(f0, W_BA), ba1 = fbits(f1, W_BA);
+            int rt = -1, rto = -1;
+            if (ba0 && ba1 && lane == 0 && !A.status) wcross_event<op>(A, P, f0, f1, ix, iy, o0, o1, out_poly, rt, rto);
+            o0 = __shfl_sync(kFull, o0, 0);
+            o1 = __shfl_sync(kFull, o1, 0);
+            rt = __shfl_sync(kFull, rt, 0);
+            if (rt >= 0) wp_redirect_all(P, __shfl_sync(kFull, A.np, 0), rt, __shfl_sync(kFull, rto, 0));
+            A.status = __shfl_sync(kFull, A.status, 0);
+            out_poly = __shfl_sync(kFull, out_poly, 0);
+            if (A.status) {
+              failed = true;
+              break;
+            }
+            // outputs above, sides flipped by the other edge's bundle
+            if (lane == l0) {
+              R.outA = o0;
+              R.fl ^= (uint32_t)ba1 << W_SIDE;
+            }
+            if (lane == l1) {
+              R.outA = o1;
+              R.fl ^= (uint32_t)ba0 << W_SIDE;
+            }
+            const unsigned tails = __ballot_sync(kFull, lane < n && fbits(R.fl, W_STA) == BUNDLE_TAIL);
+            R = wshfl(R, wswap_src(tails, fbits(f0, W_STA), l0, l1));
+          }
+          if (failed) {
             ret = kBeamsFail;
             break;
           }
-          // outputs above, sides flipped by the other edge's bundle
-          if (lane == l0) {
-            R.outA = o0;
-            R.fl ^= (uint32_t)ba1 << W_SIDE;
-          }
-          if (lane == l1) {
-            R.outA = o1;
-            R.fl ^= (uint32_t)ba0 << W_SIDE;
-          }
-          // swap the bundle of l0 (with the tails before it) and the slots up
-          // to l1: GPC steps over l0's predecessor, then over bundle tails
-          int b0 = l0;
-          if (fbits(f0, W_STA) == BUNDLE_HEAD) {
-            const unsigned tails = __ballot_sync(kFull, v2 && fbits(R.fl, W_STA) == BUNDLE_TAIL);
-            const unsigned others = ~tails & (l0 >= 1 ? (1u << (l0 - 1)) - 1u : 0u);
-            b0 = others ? 32 - __clz(others) : 0;
-          }
-          const int len2 = l1 - l0;
-          int src = lane;
-          if (lane >= b0 && lane <= l1) src = lane < b0 + len2 ? l0 + 1 + (lane - b0) : b0 + (lane - b0 - len2);
-          R = wshfl(R, src);
         } else {
           if (v2) wstore(W, lane, R);
           __syncwarp();
