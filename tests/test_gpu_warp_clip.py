@@ -1,5 +1,6 @@
 """The warp-cooperative clipper (one pair per warp, active edge table in
-shared memory) against the oracle and the reference's golden fixtures: the
+registers up to 32 edges, in shared memory beyond) against the oracle, the
+thread clipper and the reference's golden fixtures: the
 batched schedule forced to warp mode for every pair, with 256 slots and with
 32 slots (pairs whose active edge table outgrows 32 slots move it to their
 arena), and a mixed warp / thread schedule."""
@@ -193,3 +194,49 @@ def test_area_mode_warp(cuda):
     with prt.schedule(WARP):
         a1 = prt.intersection_area(LA, LB, pa, pb)
     assert torch.equal(a0, a1)
+
+
+def _spiky(n_spikes, r_in, r_out, rot=0.0, centre=(0.0, 0.0), scale=1.0):
+    a = rot + np.arange(2 * n_spikes) * np.pi / n_spikes
+    r = np.where(np.arange(2 * n_spikes) % 2 == 0, r_out, r_in) * scale
+    return np.stack([centre[0] + r * np.cos(a), centre[1] + r * np.sin(a)], 1)
+
+
+@pytest.mark.parametrize("sched", ["warp", "warp32"])
+def test_many_crossings_per_beam(cuda, sched):
+    """Spiky stars against rotated, scaled and shifted copies of themselves:
+    active edge tables of at most 32 edges with several crossings in one
+    scanbeam (the register loop's crossing table, its sort by y and the
+    bundle swaps), for all four ops; the warp clipper must give the thread
+    clipper's contours."""
+    import parlllelrtree_b200 as prt
+
+    polys_a, polys_b = [], []
+    rng = np.random.default_rng(5)
+    for k in range(48):
+        n = int(rng.integers(3, 9))
+        base = _spiky(n, 0.3, 1.0, rot=rng.uniform(0, np.pi))
+        polys_a.append([base])
+        kind = k % 4
+        if kind == 0:
+            other = _spiky(n, 0.3, 1.0, rot=rng.uniform(0.02, 0.3))
+        elif kind == 1:
+            other = _spiky(n, 0.35, 1.1, rot=rng.uniform(0, np.pi), scale=rng.uniform(0.8, 1.2))
+        elif kind == 2:
+            other = _spiky(n + 1, 0.25, 0.9, rot=rng.uniform(0, np.pi), centre=rng.uniform(-0.2, 0.2, 2))
+        else:
+            other = base[::-1].copy() * 0.97 + rng.uniform(-0.05, 0.05, 2)
+            other = other[::-1].copy()
+        polys_b.append([other])
+    A, B = _layer(polys_a), _layer(polys_b)
+    LA, LB = prt.Layer.from_dict(A), prt.Layer.from_dict(B)
+    n = len(polys_a)
+    pairs = torch.from_numpy(np.stack([np.arange(n), np.arange(n)], 1).astype(np.int32)).cuda()
+    for op in OPS:
+        plain = prt.overlay(pairs, LA, LB, op=op, sched="plain").contours()
+        got = _overlay(prt, sched, pairs, LA, LB, op=op).contours()
+        for k in range(n):
+            assert same_contours(got[k], plain[k]), (op, k)
+        for k in range(0, n, 6):
+            ref = oracle.gpc_clip(rings_of(A, k), rings_of(B, k), OPS.index(op))
+            assert same_contours(plain[k], ref), (op, k)
