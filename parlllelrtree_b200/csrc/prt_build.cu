@@ -7,6 +7,9 @@
 //   j is node j of the level below and no child pointers are stored.
 #include <cuda_runtime.h>
 
+#include <limits>
+#include <type_traits>
+
 #include <algorithm>
 #include <vector>
 #include <cstdarg>
@@ -110,25 +113,65 @@ __device__ __forceinline__ double unord_f64(unsigned long long u) {
   return __longlong_as_double((long long)u);
 }
 
-// ext[0..3] = ordered encodings of min x1, min y1, max x2, max y2 (as double)
+template <typename T>
+__device__ __forceinline__ T vmin(T a, T b) {
+  if constexpr (std::is_same<T, float>::value) return fminf(a, b);
+  else if constexpr (std::is_same<T, double>::value) return fmin(a, b);
+  else return b < a ? b : a;
+}
+template <typename T>
+__device__ __forceinline__ T vmax(T a, T b) {
+  if constexpr (std::is_same<T, float>::value) return fmaxf(a, b);
+  else if constexpr (std::is_same<T, double>::value) return fmax(a, b);
+  else return b > a ? b : a;
+}
+
+// ext[0..3] = ordered encodings of min x1, min y1, max x2, max y2 (as double).
+// The per-thread min / max run in the coordinate type (the conversion to
+// double is monotone, so the result is the same as in double).
 template <typename T>
 __global__ void extent_f64_kernel(const Box<T> *__restrict__ b, int64_t n, unsigned long long *ext) {
-  double mnx = __longlong_as_double(0x7FF0000000000000ll), mny = mnx;
-  double mxx = -mnx, mxy = -mnx;
+  T hi, lo;
+  if constexpr (std::is_floating_point<T>::value) {
+    hi = (T)__longlong_as_double(0x7FF0000000000000ll);
+    lo = -hi;
+  } else {
+    hi = std::numeric_limits<T>::max();
+    lo = std::numeric_limits<T>::lowest();
+  }
+  T tnx = hi, tny = hi, txx = lo, txy = lo;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     Box<T> x = load_box(b, i);
-    mnx = fmin(mnx, (double)x.x1);
-    mny = fmin(mny, (double)x.y1);
-    mxx = fmax(mxx, (double)x.x2);
-    mxy = fmax(mxy, (double)x.y2);
+    tnx = vmin(tnx, x.x1);
+    tny = vmin(tny, x.y1);
+    txx = vmax(txx, x.x2);
+    txy = vmax(txy, x.y2);
   }
+  double mnx = (double)tnx, mny = (double)tny, mxx = (double)txx, mxy = (double)txy;
   for (int o = 16; o; o >>= 1) {
     mnx = fmin(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
     mny = fmin(mny, __shfl_xor_sync(0xffffffffu, mny, o));
     mxx = fmax(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
     mxy = fmax(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
   }
+  // the block's warps, then one set of atomics per block (the four words
+  // are the same for every block, so fewer atomics means less contention)
+  __shared__ double red[4][32];
+  const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
   if ((threadIdx.x & 31) == 0) {
+    red[0][w] = mnx;
+    red[1][w] = mny;
+    red[2][w] = mxx;
+    red[3][w] = mxy;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < nw; k++) {
+      mnx = fmin(mnx, red[0][k]);
+      mny = fmin(mny, red[1][k]);
+      mxx = fmax(mxx, red[2][k]);
+      mxy = fmax(mxy, red[3][k]);
+    }
     atomicMin(&ext[0], ord_f64(mnx));
     atomicMin(&ext[1], ord_f64(mny));
     atomicMax(&ext[2], ord_f64(mxx));
@@ -495,7 +538,8 @@ int bu_enqueue(prt_tree *t, const void *d_boxes, const int32_t *d_ids, unsigned 
         const Box<T> *b = reinterpret_cast<const Box<T> *>(d_boxes);
         {
           PRT_PROF("extent_f64", s);
-          extent_f64_kernel<T><<<grid_for(n, 256, 4), 256, 0, s>>>(b, n, ext);
+          // 16 blocks per SM: enough loads in flight to stream the boxes
+          extent_f64_kernel<T><<<grid_for(n, 256, 16), 256, 0, s>>>(b, n, ext);
         }
         {
           PRT_PROF("morton32", s);

@@ -43,7 +43,21 @@ __global__ void __launch_bounds__(256) hist_kernel(const KeyT *__restrict__ keys
   extern __shared__ uint32_t sh[];  // passes * 256
   for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x) sh[i] = 0;
   __syncthreads();
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (sizeof(KeyT) == 4 && (reinterpret_cast<uintptr_t>(keys) & 15) == 0) {
+    // four keys per 16-byte load
+    const uint4 *k4 = reinterpret_cast<const uint4 *>(keys);
+    for (int64_t i = i0; i < n / 4; i += stride) {
+      const uint4 q = k4[i];
+      const KeyT kk[4] = {(KeyT)q.x, (KeyT)q.y, (KeyT)q.z, (KeyT)q.w};
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        for (int p = 0; p < passes; p++) atomicAdd(&sh[p * kRadix + (int)((kk[j] >> (8 * p)) & 0xFF)], 1u);
+    }
+    i0 += (n / 4) * 4;
+  }
+  for (int64_t i = i0; i < n; i += stride) {
     KeyT k = keys[i];
     for (int p = 0; p < passes; p++) atomicAdd(&sh[p * kRadix + (int)((k >> (8 * p)) & 0xFF)], 1u);
   }
