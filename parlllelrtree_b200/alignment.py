@@ -134,6 +134,7 @@ def fit_affine(A: dict, B: dict, steps: int = 200, stages=((30, 50), (10, 50), (
         sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, T_max=k_steps)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record()
+        stage_rec, stage_ov = [], []
         for it in range(k_steps):
             opt.zero_grad()
             xb = _dilate(_apply(theta, xb_all[vi]), rv, owner, float(stride))
@@ -148,12 +149,19 @@ def fit_affine(A: dict, B: dict, steps: int = 200, stages=((30, 50), (10, 50), (
             loss.backward()
             opt.step()
             sched.step()
-            records.append({"stride": stride, "parcels": m, "pairs": int(len(pairs)), "overlap": -float(loss.detach())})
+            # the overlap stays on the device (no host round trip per step)
+            # unless a logger wants it now
+            stage_rec.append({"stride": stride, "parcels": m, "pairs": int(len(pairs))})
+            stage_ov.append(-loss.detach())
             if log:
-                log(records[-1])
+                stage_rec[-1]["overlap"] = float(stage_ov[-1])
+                log(stage_rec[-1])
         ev1.record()
         ev1.synchronize()
         stage_s.append(ev0.elapsed_time(ev1) * 1e-3)
+        for r, v in zip(stage_rec, torch.stack(stage_ov).cpu().tolist()):
+            r["overlap"] = v
+        records.extend(stage_rec)
     return theta.detach().cpu().numpy(), records, stage_s
 
 
