@@ -181,13 +181,12 @@ __global__ void __launch_bounds__(128) clip_plain_kernel(PairSrc S, ClipOut O, c
 // 32 in thread mode), then steals from the smaller bins after it.  One warp
 // per block spreads the big-pair warps over every SM; the block's dynamic
 // shared memory holds the warp clipper's active-edge slots.
-// Compiled for kLptWarpsPerSM resident warps per SM (at most 168 registers a
-// thread): with fewer, the warp clipper's shuffle and FP64 latencies go
-// unhidden; with more, its register loop spills.
-__global__ void __launch_bounds__(32, kLptWarpsPerSM)
-    clip_lpt_kernel(PairSrc S, ClipOut O, const uint32_t *__restrict__ order, BinPlan plan,
-                    unsigned long long *tickets, unsigned char *arena, int scale,
-                    const int64_t *__restrict__ dyn_ranges) {
+// The body of the persistent launch; kWarp = false compiles the warp clipper
+// out (every bin in thread mode).
+template <bool kWarp>
+__device__ __forceinline__ void lpt_body(const PairSrc &S, const ClipOut &O, const uint32_t *__restrict__ order,
+                                         const BinPlan &plan, unsigned long long *tickets, unsigned char *arena,
+                                         int scale, const int64_t *__restrict__ dyn_ranges) {
   __shared__ int64_t s_begin[PRT_MAX_BINS], s_end[PRT_MAX_BINS];
   __shared__ int32_t s_mode[PRT_MAX_BINS];
   const int lane = threadIdx.x & 31;
@@ -208,7 +207,7 @@ __global__ void __launch_bounds__(32, kLptWarpsPerSM)
   unsigned long long *fallbacks = tickets + PRT_MAX_BINS;
   for (int b = g; b < nbins; b++) {
     const int64_t begin = s_begin[b], end = s_end[b];
-    if (s_mode[b]) {
+    if (kWarp && s_mode[b]) {
       for (;;) {
         unsigned long long t = 0;
         if (lane == 0) t = atomicAdd(&tickets[b], 1ull);
@@ -230,6 +229,25 @@ __global__ void __launch_bounds__(32, kLptWarpsPerSM)
       }
     }
   }
+}
+
+// Compiled for kLptWarpsPerSM resident warps per SM (at most 168 registers a
+// thread): with fewer, the warp clipper's shuffle and FP64 latencies go
+// unhidden; with more, its register loop spills.
+__global__ void __launch_bounds__(32, kLptWarpsPerSM)
+    clip_lpt_kernel(PairSrc S, ClipOut O, const uint32_t *__restrict__ order, BinPlan plan,
+                    unsigned long long *tickets, unsigned char *arena, int scale,
+                    const int64_t *__restrict__ dyn_ranges) {
+  lpt_body<true>(S, O, order, plan, tickets, arena, scale, dyn_ranges);
+}
+
+// The same launch when no bin with pairs is in warp mode: without the warp
+// clipper the thread clipper fits kLptThreadWarpsPerSM resident warps per SM,
+// which hide more of its list-walking latency.
+__global__ void __launch_bounds__(32, kLptThreadWarpsPerSM)
+    clip_lpt_thread_kernel(PairSrc S, ClipOut O, const uint32_t *__restrict__ order, BinPlan plan,
+                           unsigned long long *tickets, unsigned char *arena, int scale) {
+  lpt_body<false>(S, O, order, plan, tickets, arena, scale, nullptr);
 }
 
 // Sort keys: larger vertex counts first.
@@ -375,7 +393,7 @@ int schedule_valid(const prt_schedule &s) {
 }
 
 size_t plan_bins(const prt_schedule &sc, const int64_t *counts, const int64_t *maxnv, size_t budget, BinPlan &plan,
-                 size_t *smem, int scale) {
+                 size_t *smem, int scale, bool thread_kernel) {
   memset(&plan, 0, sizeof plan);
   plan.nbins = sc.nbins;
   plan.wcap = sc.aet_slots;
@@ -397,7 +415,11 @@ size_t plan_bins(const prt_schedule &sc, const int64_t *counts, const int64_t *m
   }
   region = (region + 511) & ~(int64_t)511;
   // no more warps than can be resident: the persistent launch must not queue
-  int64_t warps = std::min<int64_t>(work, (int64_t)kSMs * std::min(sc.warps_per_sm, kLptWarpsPerSM));
+  // (a launch without warp-mode pairs uses the thread-only kernel, whose
+  // resident limit is higher; the schedule's warps_per_sm is for the other)
+  plan.thread_only = thread_kernel && !any_warp ? 1 : 0;
+  const int per_sm = plan.thread_only ? kLptThreadWarpsPerSM : std::min(sc.warps_per_sm, kLptWarpsPerSM);
+  int64_t warps = std::min<int64_t>(work, (int64_t)kSMs * per_sm);
   warps = std::min<int64_t>(warps, (int64_t)(budget / (size_t)region));
   if (work > 0) warps = std::max<int64_t>(warps, 1);
   for (int b = 0; b <= sc.nbins; b++) plan.warp0[b] = b == 0 ? 0 : warps;
@@ -583,7 +605,7 @@ static int run_batched(OverlayState &st, const int64_t *d_idx, int64_t count, in
   int64_t counts[PRT_MAX_BINS];
   for (int b = 0; b < nb; b++) counts[b] = hb[b + 1] - hb[b];
   size_t smem = 0;
-  const size_t bytes = plan_bins(sc, counts, hm, arena_budget(), plan, &smem, scale);
+  const size_t bytes = plan_bins(sc, counts, hm, arena_budget(), plan, &smem, scale, true);
   for (int b = 0; b < nb; b++) {
     plan.begin[b] = hb[b];
     plan.end[b] = hb[b + 1];
@@ -594,7 +616,10 @@ static int run_batched(OverlayState &st, const int64_t *d_idx, int64_t count, in
   if (!rc && warps > 0) rc = dmalloc(reinterpret_cast<void **>(&arena), bytes, s);
   if (!rc && warps > 0) {
     PRT_PROF("clip_batched", s);
-    clip_lpt_kernel<<<(unsigned)warps, 32, smem, s>>>(st.S, st.O, order, plan, tickets, arena, scale, nullptr);
+    if (plan.thread_only)
+      clip_lpt_thread_kernel<<<(unsigned)warps, 32, 0, s>>>(st.S, st.O, order, plan, tickets, arena, scale);
+    else
+      clip_lpt_kernel<<<(unsigned)warps, 32, smem, s>>>(st.S, st.O, order, plan, tickets, arena, scale, nullptr);
   }
   if (!rc) {
     cudaError_t e = cudaGetLastError();

@@ -49,6 +49,8 @@ namespace prt {
 // Resident warps per SM of the persistent batched clip launch (its launch
 // bounds); a schedule's warps_per_sm is capped at it.
 constexpr int kLptWarpsPerSM = 12;
+// Resident warps per SM of the same launch when no pair is clipped by a warp.
+constexpr int kLptThreadWarpsPerSM = 24;
 
 // Bins of the batched schedule, size-descending: bin b holds sorted positions
 // [begin[b], end[b]).  Warps [warp0[g], warp0[g+1]) start on bin g with
@@ -63,7 +65,8 @@ struct BinPlan {
   int64_t arena_off[PRT_MAX_BINS];
   int32_t warp_mode[PRT_MAX_BINS];
   int nbins;
-  int wcap;  // AET slots per warp (warp mode)
+  int wcap;         // AET slots per warp (warp mode)
+  int thread_only;  // no bin with pairs in warp mode: the thread-only kernel
 };
 
 // The schedule of the calling process (prt_schedule_set).
@@ -72,9 +75,11 @@ prt_schedule current_schedule();
 int schedule_valid(const prt_schedule &s);
 // Fills plan for bins with at most counts[b] pairs of at most maxnv[b]
 // vertices, arena limited to `budget` bytes; returns the arena bytes and the
-// dynamic shared memory per block in *smem.
+// dynamic shared memory per block in *smem.  With thread_kernel, a plan with
+// no warp-mode pairs is marked for the thread-only kernel (and sized for its
+// resident warps).
 size_t plan_bins(const prt_schedule &sc, const int64_t *counts, const int64_t *maxnv, size_t budget, BinPlan &plan,
-                 size_t *smem, int scale = 1);
+                 size_t *smem, int scale = 1, bool thread_kernel = false);
 
 // Allows the persistent clip kernel `smem` bytes of dynamic shared memory.
 int prepare_lpt_launch(size_t smem);
