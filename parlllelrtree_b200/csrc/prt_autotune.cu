@@ -39,7 +39,7 @@ struct Timer {
 
 // Schedule with pairs above warp_above vertices in warp mode.
 prt_schedule make_schedule(int64_t warp_above, int slots, int warps) {
-  std::vector<int64_t> thr = {1ll << 40, 4096, 1024, 256, 64};
+  std::vector<int64_t> thr = {1ll << 40, 4096, 1024, 256, 128, 64};
   if (warp_above > 64 && warp_above < 4096) thr.push_back(warp_above);
   std::sort(thr.begin(), thr.end(), std::greater<int64_t>());
   thr.erase(std::unique(thr.begin(), thr.end()), thr.end());
@@ -167,13 +167,13 @@ int prt_autotune(const prt_layer *base, const prt_layer *overlay, int op, int64_
     out->candidates++;
     return PRT_OK;
   };
-  int64_t warp_above = 256;
+  int64_t warp_above = 128;
   int slots = 64, wps = kLptWarpsPerSM;
   prt_schedule best = make_schedule(warp_above, slots, wps);
   double best_ms = 1e30;
   if (!rc && m > 0) {
     rc = time_sched(best, &best_ms);
-    const int64_t cands_w[] = {0, 64, 1024, 1ll << 41};
+    const int64_t cands_w[] = {0, 64, 256, 1024, 1ll << 41};
     for (int64_t wa : cands_w) {
       if (rc || secs_since(t0) > time_budget_s) break;
       prt_schedule c = make_schedule(wa, slots, wps);

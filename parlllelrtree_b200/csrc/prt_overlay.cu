@@ -348,19 +348,21 @@ size_t arena_budget() {
 }  // namespace
 
 // ---- batched schedule ----------------------------------------------------------
-// Default: pairs above 256 vertices are clipped one per warp, smaller ones one
-// per thread; kLptWarpsPerSM warps per SM, what an SM holds at the clip
+// Default: pairs above 128 vertices are clipped one per warp, smaller ones one
+// per thread (32 pairs of up to 256 vertices in one warp's ticket made the
+// ticket long enough to leave a tail; below 128, one pair per thread is the
+// faster mode); kLptWarpsPerSM warps per SM, what an SM holds at the clip
 // kernel's register count; 64 shared-memory slots per warp (the warp
 // clipper keeps active edge tables of up to 32 edges in registers).
 static prt_schedule default_schedule() {
   prt_schedule d;
   memset(&d, 0, sizeof d);
-  d.nbins = 5;
+  d.nbins = 6;
   d.aet_slots = 64;
   d.warps_per_sm = kLptWarpsPerSM;
-  const int64_t thr[5] = {1ll << 40, 4096, 1024, 256, 64};
-  const int32_t wm[5] = {1, 1, 1, 0, 0};
-  for (int b = 0; b < 5; b++) {
+  const int64_t thr[6] = {1ll << 40, 4096, 1024, 256, 128, 64};
+  const int32_t wm[6] = {1, 1, 1, 1, 0, 0};
+  for (int b = 0; b < 6; b++) {
     d.bin_thresholds[b] = thr[b];
     d.bin_warp_mode[b] = wm[b];
   }
