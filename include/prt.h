@@ -149,16 +149,22 @@ int prt_join(const prt_tree *t, const void *d_queries, int coord_type, int64_t n
              prt_pair *d_pairs, int64_t cap, int64_t *h_count, void *stream);
 
 /* prt_join without any device allocation (no counterpart in the reference).
- * For callers that cannot allocate device memory when they join: inside a
- * CUDA stream capture, under a host process that owns the whole device memory
- * budget through its own pool, or in a loop that cannot afford the device
- * synchronisation an allocation may cause.  The frontier scratch lives in a
- * fixed array of the library (64 MiB + 512 B, reserved on every GPU that loads
- * the library): a level frontier above 4,194,304 (query, node) items returns
- * PRT_ERR_CAPACITY with a message, as does a pair count above `cap` (the count
- * is still reported).  The first call on a device looks the array up, so make
- * it before any stream capture.  Calls share the array: calls that can overlap
- * on the GPU race and must be serialised by the caller. */
+ * For callers that may not allocate device memory when they join: a host
+ * process whose own pool owns the whole device memory budget (a serving
+ * process or a framework allocator that treats any allocation outside its
+ * pool as a failure), or an embedding that forbids the library from calling
+ * cudaMalloc / cudaMallocAsync at all.  The frontier scratch lives in a fixed
+ * array of the library (64 MiB + 512 B, reserved on every GPU that loads the
+ * library until the process exits): a level frontier above 4,194,304
+ * (query, node) items returns PRT_ERR_CAPACITY with a message, as does a pair
+ * count above `cap` (the count is still reported).  The call waits for
+ * `stream` once at its end, to read the level and pair counts.  The first
+ * call on a device looks the array's device address up and keeps it for the
+ * process; make that first call before any stream capture, and do not call
+ * this entry point again on a device after cudaDeviceReset.  Calls share the
+ * array and its contents stay from one call to the next (the counters are
+ * cleared by every call): calls that can overlap on the GPU race and must be
+ * serialised by the caller. */
 int prt_join_noalloc(const prt_tree *t, const void *d_queries, int coord_type, int64_t nq,
                      prt_pair *d_pairs, int64_t cap, int64_t *h_count, void *stream);
 
@@ -172,6 +178,11 @@ int prt_join_sorted(const prt_tree *t, const void *d_queries, int coord_type, in
  * entries - 1) (the RtreeSearch return value), overlapping leaf entries. */
 int prt_query_counts(const prt_tree *t, const void *d_queries, int coord_type, int64_t nq,
                      int td_slots, int64_t *d_counts, void *stream);
+
+/* Pairs of overlapping sibling entries summed over every node of the tree:
+ * the reference's tree-quality digest sum3 (RtreeSearch1,
+ * BotomUp-rtree.cu:574-590, TopDown-rtree.cu:78-93). */
+int prt_tree_sibling_overlaps(const prt_tree *t, int64_t *h_count, void *stream);
 
 /* ---------------------------------------------------------------- overlay */
 
@@ -313,6 +324,14 @@ int prt_pipeline_free(prt_pipeline *p);
  * readData quantises, vector_map_overlay_gpc_kernel.cu:752-888). */
 int prt_layer_mbr(const prt_layer *layer, double *d_out, void *stream);
 
+/* The same boxes quantised as readData does before the reference builds its
+ * tree: (int)(v * scale) truncated toward zero, scale 1e5 in the reference
+ * (vector_map_overlay_gpc_kernel.cu:805-808, 845-848); n_poly x 4 int32 into
+ * device memory (values outside the int32 range saturate).  A tree built on
+ * them with PRT_COORD_I32, joined with the other layer's quantised boxes,
+ * gives the reference's candidate set. */
+int prt_layer_mbr_i32(const prt_layer *layer, double scale, int32_t *d_out, void *stream);
+
 /* Autotuner (no reference counterpart): times the build + join for fanouts
  * 8..32 and the batched clip for candidate schedules (warp-mode threshold,
  * shared-memory slots, warps per SM) on an evenly strided sample of at most
@@ -358,6 +377,19 @@ int prt_profile_enable(int mode);
 int prt_profile_focus(const char *kernel_name);
 int prt_profile_reset(void);
 int prt_profile_read(char *names, int names_cap, double *ms_total, int64_t *launches, int cap);
+
+/* ---------------------------------------------------------------- bounded waits */
+
+/* Test hook for the bounded device-side waits (no reference counterpart).
+ * Every decoupled look-back of the radix sort polls its predecessors at most
+ * `polls` times (<= 0: the built-in limit of 4,194,304) before it gives up,
+ * records a timeout and returns; the call that launched it then returns
+ * PRT_ERR_TIMEOUT.  With never_published != 0 every look-back sees no
+ * predecessor published, so each wait runs to its limit: this exercises the
+ * timeout path on a device without a hang or a fault.  Applies to the sorts
+ * launched after the call, process-wide; prt_debug_wait_limit(0, 0) restores
+ * the default. */
+int prt_debug_wait_limit(int polls, int never_published);
 
 #ifdef __cplusplus
 }

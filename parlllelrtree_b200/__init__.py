@@ -149,11 +149,18 @@ class Tree:
                                      _stream()))
         return out
 
+    def sibling_overlaps(self) -> int:
+        """Overlapping sibling-entry pairs over all nodes: the reference's
+        RtreeSearch1 digest (BotomUp-rtree.cu:574-590)."""
+        n = C.c_int64(0)
+        check(lib().prt_tree_sibling_overlaps(self._h, C.byref(n), _stream()))
+        return int(n.value)
+
     def digests(self, queries, td_slots: bool = False):
-        """The reference programs' printed digests sum, sum1, sum2 for a
-        self-join (BotomUp-rtree.cu:1023-1025)."""
+        """The reference programs' printed digests sum, sum1, sum2, sum3 for a
+        self-join (BotomUp-rtree.cu:1023-1027, TopDown-rtree.cu:794-798)."""
         c = self.query_counts(queries, td_slots).cpu().numpy()
-        return int(c[:, 0].sum()), int(c[:, 1].sum()), int(c[:, 2].sum()) // 2
+        return int(c[:, 0].sum()), int(c[:, 1].sum()), int(c[:, 2].sum()) // 2, self.sibling_overlaps()
 
 
 def _build(fn, boxes, *args):
@@ -210,20 +217,22 @@ class Layer:
         return _LayerStruct(self.poly_ring.data_ptr(), self.ring_vert.data_ptr(), self.ring_hole.data_ptr(),
                             x.data_ptr(), self.n_poly)
 
-    def mbr(self) -> torch.Tensor:
-        """float64 [P, 4] polygon bounding boxes (x1, y1, x2, y2)."""
-        xy = self.xy
-        vstart = self.ring_vert[self.poly_ring[:-1]]
-        vend = self.ring_vert[self.poly_ring[1:]]
-        owner = torch.repeat_interleave(torch.arange(self.n_poly, device=xy.device), vend - vstart)
-        out = torch.empty((self.n_poly, 4), dtype=torch.float64, device=xy.device)
-        inf = torch.finfo(torch.float64).max
-        out[:, 0:2] = inf
-        out[:, 2:4] = -inf
-        out[:, 0].scatter_reduce_(0, owner, xy[vstart[0]:vend[-1], 0], "amin")
-        out[:, 1].scatter_reduce_(0, owner, xy[vstart[0]:vend[-1], 1], "amin")
-        out[:, 2].scatter_reduce_(0, owner, xy[vstart[0]:vend[-1], 0], "amax")
-        out[:, 3].scatter_reduce_(0, owner, xy[vstart[0]:vend[-1], 1], "amax")
+    def mbr(self, xy: torch.Tensor | None = None) -> torch.Tensor:
+        """float64 [P, 4] polygon bounding boxes (x1, y1, x2, y2) over all
+        rings (prt_layer_mbr), optionally for replacement coordinates xy."""
+        out = torch.empty((self.n_poly, 4), dtype=torch.float64, device=self.xy.device)
+        s = self.struct(xy)
+        check(lib().prt_layer_mbr(C.byref(s), _ptr(out), _stream()))
+        return out
+
+    def mbr_quantised(self, scale: float = 1e5, xy: torch.Tensor | None = None) -> torch.Tensor:
+        """int32 [P, 4] polygon bounding boxes quantised as the reference's
+        readData does, (int)(v * scale) truncated toward zero
+        (vector_map_overlay_gpc_kernel.cu:805-808, 845-848); a tree built on
+        them (PRT_COORD_I32) gives the reference's candidate set."""
+        out = torch.empty((self.n_poly, 4), dtype=torch.int32, device=self.xy.device)
+        s = self.struct(xy)
+        check(lib().prt_layer_mbr_i32(C.byref(s), C.c_double(scale), _ptr(out), _stream()))
         return out
 
 

@@ -44,6 +44,7 @@ _SIGS = {
     "prt_join_sorted": (_I, [_P, _P, _I, _I64, _P, _I64, _P, _P]),
     "prt_join_noalloc": (_I, [_P, _P, _I, _I64, _P, _I64, _P, _P]),
     "prt_query_counts": (_I, [_P, _P, _I, _I64, _I, _P, _P]),
+    "prt_tree_sibling_overlaps": (_I, [_P, _P, _P]),
     "prt_overlay_run": (_I, [_P, _I64, C.c_int32, _P, _P, _P, _I, _I, _P, _P]),
     "prt_overlay_run_ref": (_I, [_P, _I64, C.c_int32, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _P, _I64, _I, _I,
                                  _P, _P]),
@@ -56,6 +57,7 @@ _SIGS = {
     "prt_schedule_set": (_I, [_P]),
     "prt_schedule_get": (_I, [_P]),
     "prt_layer_mbr": (_I, [_P, _P, _P]),
+    "prt_layer_mbr_i32": (_I, [_P, C.c_double, _P, _P]),
     "prt_autotune": (_I, [_P, _P, _I, _I64, C.c_double, _P, _P]),
     "prt_pipeline_create": (_I, [_P, _P, _P, _P]),
     "prt_pipeline_run": (_I, [_P, _P]),
@@ -65,6 +67,7 @@ _SIGS = {
     "prt_pipeline_free": (_I, [_P]),
     "prt_area_fwd": (_I, [_P, _P, _I64, _P, _P, _P, _P]),
     "prt_area_bwd": (_I, [_P, _P, _I64, _P, _P, _P, _P, _P, _P]),
+    "prt_debug_wait_limit": (_I, [_I, _I]),
     "prt_profile_enable": (_I, [_I]),
     "prt_profile_focus": (_I, [C.c_char_p]),
     "prt_profile_reset": (_I, []),

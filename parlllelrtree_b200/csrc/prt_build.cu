@@ -301,6 +301,7 @@ __global__ void td_key32_kernel(const Box<T> *__restrict__ b, const uint32_t *__
                                 int64_t seg, int use_y, uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     uint32_t r = perm ? perm[i] : (uint32_t)i;
+    if ((int64_t)r >= n) r = 0;  // only after a timed-out sort (reported by the caller)
     Box<T> x = load_box(b, r);
     uint32_t c = ukey(use_y ? x.y1 : x.x1);
     keys[i] = ((uint64_t)(i / seg) << 32) | c;
@@ -314,6 +315,7 @@ __global__ void td_key64_kernel(const Box<T> *__restrict__ b, const uint32_t *__
                                 int use_y, uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     uint32_t r = perm ? perm[i] : (uint32_t)i;
+    if ((int64_t)r >= n) r = 0;  // only after a timed-out sort (reported by the caller)
     Box<T> x = load_box(b, r);
     keys[i] = ukey(use_y ? x.y1 : x.x1);
     vals[i] = (uint32_t)i;
@@ -329,8 +331,11 @@ __global__ void td_segkey_kernel(const uint32_t *__restrict__ pos, int64_t n, in
 
 __global__ void gather_u32_kernel(const uint32_t *__restrict__ src, const uint32_t *__restrict__ idx, int64_t n,
                                   uint32_t *__restrict__ dst) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    dst[i] = src ? src[idx[i]] : idx[i];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t k = idx[i];
+    if ((int64_t)k >= n) k = 0;  // only after a timed-out sort (reported by the caller)
+    dst[i] = src ? src[k] : k;
+  }
 }
 
 __global__ void select_copy_u32_kernel(const uint32_t *a, const uint32_t *b, const int *sel, int64_t n,
@@ -358,6 +363,7 @@ __global__ void pack_leaf_kernel(const Box<T> *__restrict__ b, const int32_t *__
     Box<T> x = empty_box<T>();
     if (j < n) {
       uint32_t r = perm[j];
+      if ((int64_t)r >= n) r = 0;  // only after a timed-out sort (reported by the caller)
       x = load_box(b, r);
       leaf_id[j] = ids ? ids[r] : (int32_t)r;
       leaf_perm[j] = (int32_t)r;

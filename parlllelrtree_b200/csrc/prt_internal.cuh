@@ -35,6 +35,16 @@ enum : unsigned { kErrCapacity = 1u, kErrTimeout = 2u, kErrInvalid = 4u };
 // CTA's flag gives up after this many polls and records kErrTimeout.
 constexpr int kSpinLimit = 1 << 22;
 
+// The wait limit the next sorts use: kSpinLimit polls unless a test lowered
+// it with prt_debug_wait_limit, which can also make every look-back see no
+// predecessor published, so that each wait runs to its limit and the
+// timeout path is exercised without a hang or a fault.
+struct WaitLimit {
+  int polls;
+  int blind;
+};
+WaitLimit wait_limit();
+
 constexpr int kSMs = 148;
 
 // ---- launch profiler ---------------------------------------------------------

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 #include "prt_internal.cuh"
@@ -136,8 +137,41 @@ int launch_expand(const JoinLevel &J, const void *queries, int fanout, cudaStrea
   return PRT_OK;
 }
 
-// Frontier capacity that worked last time (grows across calls).
-int64_t g_frontier_hint = 1 << 20;
+// Overlapping pairs of sibling entries (the reference's RtreeSearch1,
+// BotomUp-rtree.cu:574-590, TopDown-rtree.cu:78-93): for every node of every
+// level, the entry pairs j < i < fill whose boxes intersect.  One warp per
+// node, lane i holds entry i and counts its overlaps with the entries before
+// it, which it receives by shuffles; one atomic per warp.
+template <typename T>
+__global__ void __launch_bounds__(256) sibling_kernel(const Box<T> *__restrict__ lv, int64_t n_entries, int fanout,
+                                                      unsigned long long *__restrict__ total) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nodes = (n_entries + fanout - 1) / fanout;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long acc = 0;
+  for (int64_t node = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; node < nodes; node += nw) {
+    const int64_t first = node * fanout;
+    const int fill = (int)min((int64_t)fanout, n_entries - first);
+    Box<T> b = empty_box<T>();
+    if (lane < fill) b = load_box(lv, first + lane);
+    unsigned c = 0;
+    for (int j = 0; j < fill - 1; j++) {
+      Box<T> o;
+      o.x1 = __shfl_sync(0xffffffffu, b.x1, j);
+      o.y1 = __shfl_sync(0xffffffffu, b.y1, j);
+      o.x2 = __shfl_sync(0xffffffffu, b.x2, j);
+      o.y2 = __shfl_sync(0xffffffffu, b.y2, j);
+      c += (j < lane && lane < fill && overlaps(b, o)) ? 1u : 0u;
+    }
+    acc += c;
+  }
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0 && acc) atomicAdd(total, acc);
+}
+
+// Frontier capacity that worked last time (grows across calls; shared by the
+// process's threads, so it is atomic).
+std::atomic<int64_t> g_frontier_hint{1 << 20};
 
 // Runs the traversal.  pairs may be nullptr with cap 0 (count only).
 int run_join(const prt_tree *t, const void *d_queries, int coord, int64_t nq, uint2 *d_pairs, int64_t cap,
@@ -151,7 +185,7 @@ int run_join(const prt_tree *t, const void *d_queries, int coord, int64_t nq, ui
   if (nq == 0) return PRT_OK;
   const TreeLevels &L = t->lv;
   const size_t bs = 4 * coord_size(t->coord);
-  int64_t fcap = std::max<int64_t>(g_frontier_hint, 4 * nq);
+  int64_t fcap = std::max<int64_t>(g_frontier_hint.load(std::memory_order_relaxed), 4 * nq);
   for (int attempt = 0; attempt < 8; attempt++) {
     unsigned long long *cnt = nullptr;
     uint2 *fr[2] = {nullptr, nullptr};
@@ -208,7 +242,9 @@ int run_join(const prt_tree *t, const void *d_queries, int coord, int64_t nq, ui
     for (int l = 1; l < L.levels; l++) worst = std::max(worst, h[l]);
     if ((int64_t)worst > fcap) {
       fcap = (int64_t)(worst + worst / 4 + 1024);
-      g_frontier_hint = std::max(g_frontier_hint, fcap);
+      int64_t seen = g_frontier_hint.load(std::memory_order_relaxed);
+      while (seen < fcap && !g_frontier_hint.compare_exchange_weak(seen, fcap, std::memory_order_relaxed)) {
+      }
       continue;
     }
     int64_t np = (int64_t)h[PRT_MAX_LEVELS];
@@ -303,28 +339,60 @@ int prt_query_counts(const prt_tree *t, const void *d_queries, int coord_type, i
                   reinterpret_cast<cudaStream_t>(stream));
 }
 
+int prt_tree_sibling_overlaps(const prt_tree *t, int64_t *h_count, void *stream) {
+  PRT_CHECK(t && h_count, PRT_ERR_INVALID, "NULL argument");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  *h_count = 0;
+  unsigned long long *d = nullptr;
+  int rc = dalloc(&d, 1, s);
+  if (rc) return rc;
+  cudaError_t e = cudaMemsetAsync(d, 0, 8, s);
+  const size_t bs = 4 * coord_size(t->coord);
+  for (int l = 0; l < t->lv.levels && e == cudaSuccess; l++) {
+    const int64_t nodes = (t->lv.count[l] + t->fanout - 1) / t->fanout;
+    const void *lv = reinterpret_cast<const char *>(t->d_mbr) + t->lv.offset[l] * bs;
+    rc = dispatch_coord(t->coord, [&](auto tag) {
+      using T = decltype(tag);
+      PRT_PROF("sibling", s);
+      sibling_kernel<T><<<grid_for(nodes * 32, 256, 8), 256, 0, s>>>(reinterpret_cast<const Box<T> *>(lv),
+                                                                     t->lv.count[l], t->fanout, d);
+      return PRT_OK;
+    });
+    e = cudaGetLastError();
+  }
+  unsigned long long h = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, 8, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  dfree(d, s);
+  if (e != cudaSuccess) return cuda_status(e, "sibling overlaps");
+  *h_count = (int64_t)h;
+  return rc;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
 // Allocation-free join.
 //
 // prt_join takes its frontier buffers and level counters from the
-// stream-ordered allocator.  Some callers cannot allocate device memory at
-// the moment they join: a caller in the middle of a CUDA stream capture (the
-// graph would record the allocation, or the capture mode forbids it), a host
-// process that hands the whole device budget to its own pool and treats any
-// other allocation as a failure, or a latency-critical loop that cannot take
-// the device synchronisation cudaMalloc/cudaFree may imply.  prt_join_noalloc
-// runs the same breadth-first traversal with its scratch in the file-scope
-// array below instead: the caller passes the queries and the pair buffer,
-// and the library allocates nothing.
+// stream-ordered allocator.  Some callers may not allocate device memory at
+// the moment they join: a host process that hands the whole device budget to
+// its own pool and treats any other allocation as a failure, or an embedding
+// that forbids the library from calling cudaMalloc / cudaMallocAsync at all.
+// prt_join_noalloc runs the same breadth-first traversal with its scratch in
+// the file-scope array below instead: the caller passes the queries and the
+// pair buffer, and the library allocates nothing.  The call still waits for
+// its stream once, at the end, to read the level and pair counts.
 //
 // The array is reserved on every GPU that loads the library, for the life of
 // the process.  Its device address is looked up once per device
 // (cudaGetSymbolAddress, with that device current) on the first call made
-// there, so make that first call before any stream capture.  All calls on a
-// device share the one array: calls that can overlap on the GPU (different
-// streams, or host threads) race on it and must be serialised by the caller.
+// there and kept for the process, so make that first call before any stream
+// capture, and do not call again on a device after cudaDeviceReset (the kept
+// address would be stale).  All calls on a device share the one array and its
+// contents stay from one call to the next (every call clears the counters):
+// calls that can overlap on the GPU (different streams, or host threads) race
+// on it and must be serialised by the caller.
 #include <mutex>
 
 namespace prt {

@@ -214,7 +214,8 @@ __device__ __forceinline__ void lpt_body(const PairSrc &S, const ClipOut &O, con
         t = __shfl_sync(0xffffffffu, t, 0);
         const int64_t k = begin + (int64_t)t;
         if (k >= end) break;
-        process_pair_warp(S, O, (int64_t)order[k], region, scale, W, fallbacks);
+        const int64_t i = (int64_t)order[k];
+        if (i < plan.n_pairs) process_pair_warp(S, O, i, region, scale, W, fallbacks);
       }
     } else {
       for (;;) {
@@ -224,7 +225,7 @@ __device__ __forceinline__ void lpt_body(const PairSrc &S, const ClipOut &O, con
         const int64_t k0 = begin + (int64_t)base;
         if (k0 >= end) break;
         const int64_t k = k0 + lane;
-        if (k < end) process_pair(S, O, (int64_t)order[k], slice, scale);
+        if (k < end && (int64_t)order[k] < plan.n_pairs) process_pair(S, O, (int64_t)order[k], slice, scale);
         __syncwarp();
       }
     }
@@ -283,8 +284,12 @@ __global__ void bin_bounds_kernel(const uint32_t *__restrict__ k0, const uint32_
 __global__ void select_u32_kernel(const uint32_t *a, const uint32_t *b, const int *sel, int64_t n, uint32_t *dst,
                                   const int64_t *__restrict__ idx = nullptr) {
   const uint32_t *src = *sel ? b : a;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    dst[i] = idx ? (uint32_t)idx[src[i]] : src[i];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = src[i];
+    // a timed-out sort can leave any value here: out-of-range positions are
+    // marked, skipped by the clip, and the caller reports the timeout
+    dst[i] = (int64_t)k >= n ? 0xFFFFFFFFu : idx ? (uint32_t)idx[k] : k;
+  }
 }
 
 __global__ void area_from_results_kernel(const int64_t *__restrict__ pair_cstart, const int32_t *__restrict__ pair_ncont,
@@ -596,10 +601,16 @@ static int run_batched(OverlayState &st, const int64_t *d_idx, int64_t count, in
       PRT_PROF("bin_bounds", s);
       bin_bounds_kernel<<<1, 32, 0, s>>>(k0, k1, sel, n, thr, nb, bnd, mx);
     }
+    unsigned herr = 0;
     cudaMemcpyAsync(hb, bnd, sizeof(int64_t) * nb, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(hm, mx, sizeof(int64_t) * nb, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&herr, err, sizeof herr, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) rc = cuda_status(e, "overlay batched");
+    if (!rc && (herr & kErrTimeout)) {
+      set_error("overlay batched: size sort look-back wait timed out");
+      rc = PRT_ERR_TIMEOUT;
+    }
   }
   // bin b covers sorted positions [bnd[b], bnd[b+1]) (bnd[nbins] = n)
   hb[nb] = n;
@@ -608,6 +619,7 @@ static int run_batched(OverlayState &st, const int64_t *d_idx, int64_t count, in
   for (int b = 0; b < nb; b++) counts[b] = hb[b + 1] - hb[b];
   size_t smem = 0;
   const size_t bytes = plan_bins(sc, counts, hm, arena_budget(), plan, &smem, scale, true);
+  plan.n_pairs = st.n;
   for (int b = 0; b < nb; b++) {
     plan.begin[b] = hb[b];
     plan.end[b] = hb[b + 1];

@@ -64,6 +64,7 @@ struct BinPlan {
   int64_t region[PRT_MAX_BINS];
   int64_t arena_off[PRT_MAX_BINS];
   int32_t warp_mode[PRT_MAX_BINS];
+  int64_t n_pairs;  // pair indices in the order array are below this (others are skipped)
   int nbins;
   int wcap;         // AET slots per warp (warp mode)
   int thread_only;  // no bin with pairs in warp mode: the thread-only kernel

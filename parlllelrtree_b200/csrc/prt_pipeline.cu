@@ -21,25 +21,44 @@
 namespace prt {
 namespace {
 
-// Bounding box (x1, y1, x2, y2) of every polygon over all its rings.
-__global__ void poly_mbr_kernel(LayerDev L, double *__restrict__ out) {
-  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < L.n_poly;
-       p += (int64_t)gridDim.x * blockDim.x) {
+// Bounding box (x1, y1, x2, y2) of every polygon over all its rings, one warp
+// per polygon: the lanes read the vertex array in coalesced 16-byte (x, y)
+// loads and reduce by shuffles.  A polygon without vertices gets the empty box
+// (DBL_MAX, DBL_MAX, -DBL_MAX, -DBL_MAX).  With Out = int32_t the box is
+// quantised as the reference's readData does, (int)(v * scale) truncated
+// toward zero (vector_map_overlay_gpc_kernel.cu:805-808, 845-848); values
+// outside the int32 range saturate.
+template <typename Out>
+__global__ void poly_mbr_kernel(LayerDev L, double scale, Out *__restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t p = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; p < L.n_poly; p += nw) {
     const int64_t v0 = L.ring_vert[L.poly_ring[p]], v1 = L.ring_vert[L.poly_ring[p + 1]];
     double x1 = 1.7976931348623157e308, y1 = x1, x2 = -x1, y2 = -x1;
-    for (int64_t v = v0; v < v1; v++) {
-      const double x = L.xy[2 * v], y = L.xy[2 * v + 1];
-      x1 = fmin(x1, x);
-      y1 = fmin(y1, y);
-      x2 = fmax(x2, x);
-      y2 = fmax(y2, y);
+    const bool aligned = (reinterpret_cast<uintptr_t>(L.xy) & 15) == 0;
+    const double2 *xy = reinterpret_cast<const double2 *>(L.xy);
+    for (int64_t v = v0 + lane; v < v1; v += 32) {
+      const double2 q = aligned ? __ldg(&xy[v]) : make_double2(__ldg(&L.xy[2 * v]), __ldg(&L.xy[2 * v + 1]));
+      x1 = fmin(x1, q.x);
+      y1 = fmin(y1, q.y);
+      x2 = fmax(x2, q.x);
+      y2 = fmax(y2, q.y);
     }
-    out[4 * p] = x1;
-    out[4 * p + 1] = y1;
-    out[4 * p + 2] = x2;
-    out[4 * p + 3] = y2;
+    for (int o = 16; o; o >>= 1) {
+      x1 = fmin(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+      y1 = fmin(y1, __shfl_xor_sync(0xffffffffu, y1, o));
+      x2 = fmax(x2, __shfl_xor_sync(0xffffffffu, x2, o));
+      y2 = fmax(y2, __shfl_xor_sync(0xffffffffu, y2, o));
+    }
+    if (lane < 4) {
+      const double v = lane == 0 ? x1 : lane == 1 ? y1 : lane == 2 ? x2 : y2;
+      if constexpr (sizeof(Out) == 8) out[4 * p + lane] = (Out)v;
+      else out[4 * p + lane] = (Out)__double2int_rz(v * scale);
+    }
   }
 }
+
+inline int poly_mbr_grid(int64_t n_poly) { return grid_for(n_poly * 32, 256, 8); }
 
 // Largest vertex count of a polygon of the layer (sizes the biggest arenas).
 __global__ void max_poly_vertices_kernel(LayerDev L, unsigned long long *out) {
@@ -108,8 +127,8 @@ int enqueue_run(prt_pipeline *p, cudaStream_t s) {
   PRT_CUDA(cudaMemsetAsync(p->counters, 0, sizeof(unsigned long long) * (PRT_MAX_LEVELS + 2), s));
   {
     PRT_PROF("poly_mbr", s);
-    poly_mbr_kernel<<<grid_for(p->base.n_poly, 256, 8), 256, 0, s>>>(p->base, p->base_mbr);
-    poly_mbr_kernel<<<grid_for(p->over.n_poly, 256, 8), 256, 0, s>>>(p->over, p->over_mbr);
+    poly_mbr_kernel<double><<<poly_mbr_grid(p->base.n_poly), 256, 0, s>>>(p->base, 1.0, p->base_mbr);
+    poly_mbr_kernel<double><<<poly_mbr_grid(p->over.n_poly), 256, 0, s>>>(p->over, 1.0, p->over_mbr);
   }
   int rc = bu_enqueue(p->tree, p->base_mbr, nullptr, p->build_err, s);
   if (!rc)
@@ -237,6 +256,7 @@ int prt_pipeline_create(const prt_layer *base, const prt_layer *overlay, const p
       mx[b] = std::min<int64_t>(sched.bin_thresholds[b], max_pair);
     }
     G.arena_bytes = plan_bins(sched, counts, mx, budget, G.plan, &G.smem);
+    G.plan.n_pairs = G.cap_pairs;
     rc = prepare_lpt_launch(G.smem);
     if (!rc) rc = alloc(&G.arena, G.arena_bytes);
   }
@@ -260,7 +280,21 @@ int prt_layer_mbr(const prt_layer *layer, double *d_out, void *stream) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   {
     PRT_PROF("poly_mbr", s);
-    poly_mbr_kernel<<<grid_for(layer->n_poly, 256, 8), 256, 0, s>>>(layer_dev(layer), d_out);
+    poly_mbr_kernel<double><<<poly_mbr_grid(layer->n_poly), 256, 0, s>>>(layer_dev(layer), 1.0, d_out);
+  }
+  PRT_CUDA(cudaGetLastError());
+  return PRT_OK;
+}
+
+int prt_layer_mbr_i32(const prt_layer *layer, double scale, int32_t *d_out, void *stream) {
+  PRT_CHECK(layer && d_out, PRT_ERR_INVALID, "NULL argument");
+  PRT_CHECK(layer->n_poly >= 0, PRT_ERR_INVALID, "n_poly %lld", (long long)layer->n_poly);
+  PRT_CHECK(scale > 0.0, PRT_ERR_INVALID, "scale %g", scale);
+  if (layer->n_poly == 0) return PRT_OK;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  {
+    PRT_PROF("poly_mbr", s);
+    poly_mbr_kernel<int32_t><<<poly_mbr_grid(layer->n_poly), 256, 0, s>>>(layer_dev(layer), scale, d_out);
   }
   PRT_CUDA(cudaGetLastError());
   return PRT_OK;

@@ -13,6 +13,8 @@
 // original order within a warp, then warp order, then tile order.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "prt_internal.cuh"
 
 namespace prt {
@@ -121,7 +123,7 @@ __global__ void __launch_bounds__(kSortBlock, 4) onesweep_pass(KeyT *keys0, uint
                                                            const PassPlan *__restrict__ plan,
                                                            const uint32_t *__restrict__ goff,
                                                            uint32_t *status, unsigned *tile_ticket,
-                                                           unsigned *err) {
+                                                           unsigned *err, WaitLimit wl) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   PassSmem<KeyT> &S = *reinterpret_cast<PassSmem<KeyT> *>(smem_raw);
   const PassPlan pp = *plan;
@@ -246,7 +248,7 @@ __global__ void __launch_bounds__(kSortBlock, 4) onesweep_pass(KeyT *keys0, uint
       for (int j = 0; j < kLookBatch; j++) {
         uint32_t sj = 2u << 30;  // before tile 0: an empty prefix (never reached)
         if (t - j >= 0) sj = *reinterpret_cast<volatile uint32_t *>(status + (int64_t)(t - j) * kRadix + d);
-        s[j] = sj;
+        s[j] = wl.blind ? 0u : sj;
       }
       int used = 0;
       bool done = false;
@@ -261,7 +263,7 @@ __global__ void __launch_bounds__(kSortBlock, 4) onesweep_pass(KeyT *keys0, uint
       }
       if (done) break;
       t -= used;
-      if (used == 0 && ++spins > kSpinLimit) {
+      if (used == 0 && ++spins > wl.polls) {
         timed_out = true;
         break;
       }
@@ -277,12 +279,16 @@ __global__ void __launch_bounds__(kSortBlock, 4) onesweep_pass(KeyT *keys0, uint
   // 4. write the staged tile out in coalesced runs per digit
   int64_t valid = n - base;
   if (valid > kTile) valid = kTile;
+  // (a look-back that timed out leaves the offsets wrong: the bound keeps
+  // every write inside the buffers, and the caller reports the timeout)
   for (int i = tid; i < valid; i += kSortBlock) {
     KeyT kk = S.keys[i];
     int dd = (int)((kk >> shift) & 0xFF);
     const uint32_t dst = S.global_start[dd] + (uint32_t)i;
-    dst_k[dst] = kk;
-    dst_v[dst] = S.vals[i];
+    if ((int64_t)dst < n) {
+      dst_k[dst] = kk;
+      dst_v[dst] = S.vals[i];
+    }
   }
 }
 
@@ -336,12 +342,13 @@ int radix_sort_pairs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1,
       e = cudaFuncSetAttribute(onesweep_pass<KeyT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e == cudaSuccess && dev >= 0 && dev < 256) attr_done[dev] = true;
     }
+    const WaitLimit wl = wait_limit();
     for (int p = 0; p < passes && e == cudaSuccess; p++) {
       {
         PRT_PROF("onesweep_pass", s);
         onesweep_pass<KeyT><<<(unsigned)tiles, kSortBlock, smem, s>>>(
           keys0, vals0, keys1, vals1, n, 8 * p, plan + p, goff + p * kRadix,
-          status + (size_t)p * tiles * kRadix, tick + p, d_err);
+          status + (size_t)p * tiles * kRadix, tick + p, d_err, wl);
       }
     }
     if (e == cudaSuccess) e = cudaGetLastError();
@@ -351,9 +358,23 @@ int radix_sort_pairs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1,
   return PRT_OK;
 }
 
+namespace {
+std::atomic<int> g_wait_polls{kSpinLimit};
+std::atomic<int> g_wait_blind{0};
+}  // namespace
+
+WaitLimit wait_limit() { return WaitLimit{g_wait_polls.load(), g_wait_blind.load()}; }
+
 template int radix_sort_pairs<uint32_t>(uint32_t *, uint32_t *, uint32_t *, uint32_t *, int64_t, int, int *,
                                         unsigned *, cudaStream_t);
 template int radix_sort_pairs<uint64_t>(uint64_t *, uint32_t *, uint64_t *, uint32_t *, int64_t, int, int *,
                                         unsigned *, cudaStream_t);
 
 }  // namespace prt
+
+extern "C" int prt_debug_wait_limit(int polls, int never_published) {
+  using namespace prt;
+  g_wait_polls.store(polls > 0 ? polls : kSpinLimit);
+  g_wait_blind.store(never_published ? 1 : 0);
+  return PRT_OK;
+}

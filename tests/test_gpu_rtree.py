@@ -64,7 +64,7 @@ def test_bottomup_ref64_golden(cuda, F):
     compare_bu(ex, {k: g[k] for k in ("flag", "num", "mbr", "children", "data")} | {"root": int(g["root"])})
     sh = rects - np.array([sx, sy, sx, sy])
     d = t.digests(torch.from_numpy(rects).cuda())
-    assert d == tuple(int(x) for x in g["digests"][:3])
+    assert d == tuple(int(x) for x in g["digests"][:4])
 
 
 @pytest.mark.parametrize("F", [10, 16, 32])
@@ -76,7 +76,7 @@ def test_topdown_golden(cuda, F):
     t = prt.build_topdown(torch.from_numpy(rects).cuda(), fanout=F)
     compare_td(t.export_td(), {k: g[k] for k in ("nodes_index", "nodes_mbr", "offsets")})
     d = t.digests(torch.from_numpy(rects).cuda(), td_slots=True)
-    assert d == tuple(int(x) for x in g["digests"][:3])
+    assert d == tuple(int(x) for x in g["digests"][:4])
 
 
 @pytest.mark.parametrize("kind", ["f32", "f64", "i64", "i32"])

@@ -1,6 +1,6 @@
-"""prt_join_noalloc: the join for callers that cannot allocate device memory
-(during a stream capture, under a host that owns the device memory budget, or
-where an allocation's implicit synchronisation is not acceptable).  It keeps
+"""prt_join_noalloc: the join for callers that may not allocate device memory
+(a host whose own pool owns the device memory budget and rejects any other
+allocation, or an embedding that forbids the library's cudaMalloc calls).  It keeps
 its scratch in a fixed array inside the library, so these tests call it
 through the C ABI and compare its pairs with prt_join's on two calls in a row
 (the second call must not see the first call's leftovers), and check that a
