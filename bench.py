@@ -429,10 +429,17 @@ def secondary(prt, boxes, flush, world):
     res["join_1M_windows_queries_s"] = N_WINDOWS / (ms * 1e-3)
     res["join_1M_windows_pairs_s"] = npairs / (ms * 1e-3)
     res["join_1M_windows_pairs"] = npairs
+    # join roofline: 20 B per entry examined (the reference's `num` counter),
+    # 16 B per query box, 8 B per emitted pair
+    examined = int(tree.query_counts(win)[:, 0].sum())
+    algo = 20 * examined + 16 * N_WINDOWS + 8 * npairs
+    peak, kind = hbm_peak()
+    res["join_roofline"] = {"bound": "hbm", "achieved": algo / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                            "frac": algo / (ms * 1e-3) / 1e9 / peak, "peak_source": kind,
+                            "algorithmic_bytes": algo, "entries_examined": examined, "ms": ms}
 
-    # the batched uneven overlay at a tenth of its size (1M x 1M takes ~10 min
-    # with the plain schedule; its numbers are in the design notes)
-    res["uneven_overlay_0.1"] = batched_overlay(prt, 0.1)
+    # the batched uneven overlay at its full size (1M x 1M polygons)
+    res["uneven_overlay_1.0"] = batched_overlay(prt, 1.0)
     # the differentiable-area configuration at full size
     res["differentiable_area_1M"] = differentiable_area(prt, 1_000_000)
     # the map-alignment loop, 200k parcels x 200 steps
@@ -504,13 +511,16 @@ def differentiable_area(prt, n: int = 1_000_000, reps: int = 5):
         return float(np.median(ms))
 
     f_ms = timed(fwd)
+    fb = C.c_int64(0)
+    _lib.check(L.prt_area_fwd_fallbacks(C.byref(fb)))
     b_ms = timed(bwd)
     nv = int(len(LA.xy) + len(LB.xy))
     algo = 32 * nv + 16 * n
     peak, kind = hbm_peak()
     achieved = algo / (b_ms * 1e-3) / 1e9
     return {"pairs": n, "vertices": nv, "loss": float(area.sum()),
-            "fwd_ms": f_ms, "fwd_pairs_s": n / (f_ms * 1e-3), "bwd_ms": b_ms, "bwd_pairs_s": n / (b_ms * 1e-3),
+            "fwd_ms": f_ms, "fwd_pairs_s": n / (f_ms * 1e-3), "fwd_gpc_fallback_pairs": int(fb.value),
+            "bwd_ms": b_ms, "bwd_pairs_s": n / (b_ms * 1e-3),
             "bwd_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_source": kind, "algorithmic_bytes": algo}}
 
@@ -534,49 +544,69 @@ def alignment(n: int = 200_000):
             "final_overlap": rec[-1]["overlap"]}
 
 
-def _cpu_overlay_sample(LA, LB, pairs, l2p, sample: int = 400, budget_s: float = 20.0):
-    """CPU baseline of the clip: the GPC restatement in oracle/ (C, one
-    thread) on an evenly strided sample of the candidate pairs, within a time
-    budget.  The reference's own CPU clip core (oracle/_ref) overflows its
-    fixed stack[400] on pairs with thousands of vertices, so the port stands
-    in for it here."""
-    import oracle
+def _oracle_rings(L, i):
+    pr = L.poly_ring[i:i + 2].cpu().numpy()
+    rv = L.ring_vert[pr[0]:pr[1] + 1].cpu().numpy()
+    xy = L.xy[rv[0]:rv[-1]].cpu().numpy()
+    return [xy[rv[k] - rv[0]:rv[k + 1] - rv[0]] for k in range(len(rv) - 1)]
 
+
+def _overlay_sample(LA, LB, pairs, l2p, sample: int = 400):
+    """An evenly strided sample of the candidate pairs: their positions and
+    both polygons' rings (host copies) for the CPU clip."""
     n = len(pairs)
     step = max(1, n // sample)
     idx = np.arange(0, n, step)[:sample]
-    p = pairs[idx].cpu().numpy()
+    p = pairs[torch_index(idx)].cpu().numpy()
     perm = l2p.cpu().numpy()
+    polys = [(_oracle_rings(LA, int(perm[a])), _oracle_rings(LB, int(b))) for a, b in p]
+    return idx, step, polys
 
-    def rings(L, i):
-        pr = L.poly_ring[i:i + 2].cpu().numpy()
-        rv = L.ring_vert[pr[0]:pr[1] + 1].cpu().numpy()
-        xy = L.xy[rv[0]:rv[-1]].cpu().numpy()
-        return [xy[rv[k] - rv[0]:rv[k + 1] - rv[0]] for k in range(len(rv) - 1)]
 
-    polys = [(rings(LA, int(perm[a])), rings(LB, int(b))) for a, b in p]
+def torch_index(idx):
+    import torch
+
+    return torch.from_numpy(np.asarray(idx, dtype=np.int64)).cuda()
+
+
+def _cpu_overlay_sample(polys, n, step, budget_s: float = 20.0):
+    """CPU baseline of the clip: the GPC restatement in oracle/ (C, one
+    thread) on the strided sample, within a time budget.  The reference's own
+    CPU clip core (oracle/_ref) overflows its fixed stack[400] on pairs with
+    thousands of vertices, so the port stands in for it here.  Returns the
+    baseline record and the clipped contours (for the parity check)."""
+    import oracle
+
     t0 = time.perf_counter()
-    done = 0
+    out = []
     for s_, c_ in polys:
-        oracle.gpc_clip(s_, c_, 1)
-        done += 1
+        out.append(oracle.gpc_clip(s_, c_, 1))
         if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
-    return {"value": done / dt, "unit": "pairs/s", "cores": 1, "kind": "port",
-            "sample": f"{done} of {n} candidate pairs (every {step}th), GPC restatement in oracle/ (C), one thread"}
+    return {"value": len(out) / dt, "unit": "pairs/s", "cores": 1, "kind": "port",
+            "sample": f"{len(out)} of {n} candidate pairs (every {step}th), GPC restatement in oracle/ (C), "
+                      "one thread"}, out
 
 
-def batched_overlay(prt, scale: float = 1.0, reps: int = 1, pipeline: bool = True):
+def _same(a, b):
+    return len(a) == len(b) and all(h1 == h2 and np.array_equal(v1, v2) for (h1, v1), (h2, v2) in zip(a, b))
+
+
+def batched_overlay(prt, scale: float = 1.0, plain_stride: int = 32):
     """The batched uneven overlay configuration: two layers of `scale` x 1M
     star polygons (vertex count clip(Zipf(1.2), 4, 4096), 5% with 1-3 clockwise
     holes, centres from the 64-Gaussian mixture, radius log-uniform
     6.5e-5..6.5e-4, calibrated for ~4M candidate pairs at 1M x 1M), generated
     on the device; tree over layer A's MBRs (fanout 16), join layer B, clip
-    every candidate pair with the plain schedule (one thread per pair in join
-    order) and with the batched schedule, each after one untimed warm-up run
-    (CUDA events; inputs already in HBM).  With `pipeline`, the whole
-    build-join-clip graph (prt.Pipeline) is timed too, on a side stream."""
+    every candidate pair with the batched schedule (CUDA events; inputs in
+    HBM; after an untimed warm-up on a 1% strided subset that sizes the
+    allocator pools), and the whole build-join-clip graph (prt.Pipeline) on a
+    side stream.  The plain schedule (one thread per pair in join order) is
+    timed on an evenly strided subset (every plain_stride-th pair, labelled):
+    on the full list it takes ~8 minutes.  Parity: 400 evenly strided pairs of
+    the batched results against the oracle's GPC clip, contour for contour and
+    bit for bit; the same pairs give the CPU baseline."""
     import torch
     from parlllelrtree_b200 import datagen as dg
 
@@ -584,11 +614,13 @@ def batched_overlay(prt, scale: float = 1.0, reps: int = 1, pipeline: bool = Tru
     A = dg.star_layer_device(n, seed=101, r_lo=6.5e-5, r_hi=6.5e-4)
     B = dg.star_layer_device(n, seed=102, r_lo=6.5e-5, r_hi=6.5e-4)
     LA, LB = prt.Layer.from_dict(A), prt.Layer.from_dict(B)
+    del A, B
     t = prt.build_bottomup(LA.mbr(), fanout=16)
     pairs = t.join(LB.mbr())
     l2p = t.leaf_order()
-    out = {"polygons_per_layer": n, "vertices_per_layer": [int(len(A["xy"])), int(len(B["xy"]))],
-           "pairs": int(len(pairs)), "schedule": prt.get_schedule()}
+    np_ = int(len(pairs))
+    out = {"polygons_per_layer": n, "vertices_per_layer": [int(len(LA.xy)), int(len(LB.xy))],
+           "pairs": np_, "schedule": prt.get_schedule()}
     del t
 
     def timed(fn):
@@ -601,39 +633,50 @@ def batched_overlay(prt, scale: float = 1.0, reps: int = 1, pipeline: bool = Tru
         b.synchronize()
         return a.elapsed_time(b), r
 
-    for sched in ("batched", "plain"):
-        fn = lambda: prt.overlay(pairs, LA, LB, leaf_to_poly=l2p, sched=sched)
-        warm = fn()  # warm-up: allocator pools, arena pages
-        del warm
-        best, info = None, None
-        for _ in range(reps):
-            ms, r = timed(fn)
-            if best is None or ms < best:
-                best = ms
-                info = (r.nonempty, r.retried, r.n_contours, r.n_vertices)
-            del r
-        out[f"{sched}_ms"] = best
-        out[f"{sched}_pairs_s"] = len(pairs) / (best * 1e-3)
-        out[f"{sched}_nonempty"], out[f"{sched}_retried"], out[f"{sched}_contours"], out[f"{sched}_vertices"] = info
+    warm = prt.overlay(pairs[::100].contiguous(), LA, LB, leaf_to_poly=l2p, sched="batched")
+    del warm
+    ms, r = timed(lambda: prt.overlay(pairs, LA, LB, leaf_to_poly=l2p, sched="batched"))
+    out["batched_ms"] = ms
+    out["batched_pairs_s"] = np_ / (ms * 1e-3)
+    out["batched_nonempty"], out["batched_retried"] = r.nonempty, r.retried
+    out["batched_contours"], out["batched_vertices"] = r.n_contours, r.n_vertices
+    # parity on the strided sample (its CPU clip is the baseline too)
+    idx, step, polys = _overlay_sample(LA, LB, pairs, l2p)
+    got = r.contours_of(idx)
+    del r
+    base, ref = _cpu_overlay_sample(polys, np_, step)
+    mism = sum(0 if _same(g, e) else 1 for g, e in zip(got, ref))
+    out["parity_checked"], out["parity_mismatches"] = len(ref), mism
+    out["cpu_baseline"] = base
+    # plain schedule on a strided subset of the same pairs
+    sub = pairs[::plain_stride].contiguous()
+    warm = prt.overlay(sub[::10].contiguous(), LA, LB, leaf_to_poly=l2p, sched="plain")
+    del warm
+    ms_p, r = timed(lambda: prt.overlay(sub, LA, LB, leaf_to_poly=l2p, sched="plain"))
+    out["plain_sample"] = f"every {plain_stride}th candidate pair ({len(sub)} pairs), join order"
+    out["plain_ms"] = ms_p
+    out["plain_pairs_s"] = len(sub) / (ms_p * 1e-3)
+    out["plain_nonempty"] = r.nonempty
+    del r
     out["batched_over_plain"] = out["batched_pairs_s"] / out["plain_pairs_s"]
-    out["cpu_baseline"] = _cpu_overlay_sample(LA, LB, pairs, l2p)
-    if pipeline:
-        stream = torch.cuda.Stream()
-        with torch.cuda.stream(stream):
-            pipe = prt.Pipeline(LA, LB, max_pairs=int(len(pairs) * 1.25) + 1024)
-            pipe.run()  # first run: uncaptured pass + capture
-            stream.synchronize()
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            pipe.run()
-            b.record(stream)
-            b.synchronize()
-            sz = pipe.sizes()
-        out["pipeline_ms"] = a.elapsed_time(b)
-        out["pipeline_pairs_s"] = sz["pairs"] / (out["pipeline_ms"] * 1e-3)
-        out["pipeline_sizes"] = sz
-        del pipe
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        pipe = prt.Pipeline(LA, LB, max_pairs=int(np_ * 1.25) + 1024)
+        pipe.run()  # first run: uncaptured pass + capture
+        stream.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        pipe.run()
+        b.record(stream)
+        b.synchronize()
+        sz = pipe.sizes()
+    out["pipeline_ms"] = a.elapsed_time(b)
+    out["pipeline_pairs_s"] = sz["pairs"] / (out["pipeline_ms"] * 1e-3)
+    out["pipeline_sizes"] = sz
+    out["pipeline_matches_batched"] = bool(sz["pairs"] == np_ and sz["contours"] == out["batched_contours"]
+                                           and sz["vertices"] == out["batched_vertices"])
+    del pipe
     return out
 
 

@@ -232,6 +232,15 @@ int prt_results_device(const prt_results *r, const int64_t **pair_cont_start,
  * [pairs+1], h_cont_nverts / h_cont_hole [contours], h_xy [2*vertices]. */
 int prt_results_copy(const prt_results *r, int64_t *h_pair_cont_off, int32_t *h_cont_nverts,
                      int32_t *h_cont_hole, double *h_xy);
+/* Copies the results of the k pairs listed in h_pairs (pair indices) to host
+ * buffers in list order: h_pair_cont_off [k+1], h_cont_nverts / h_cont_hole
+ * [cont_cap], h_xy [2 * vert_cap].  h_need[0..1] receives the contours and
+ * vertices needed; PRT_ERR_CAPACITY (nothing copied) when they exceed the
+ * caps.  For checking or exporting a few pairs of a result set too large for
+ * host memory (no reference counterpart). */
+int prt_results_copy_pairs(const prt_results *r, const int64_t *h_pairs, int64_t k, int64_t *h_pair_cont_off,
+                           int32_t *h_cont_nverts, int32_t *h_cont_hole, double *h_xy, int64_t cont_cap,
+                           int64_t vert_cap, int64_t *h_need);
 /* Per-pair intersection area of the results (hole contours negative). */
 int prt_results_area(const prt_results *r, double *d_area, void *stream);
 int prt_results_free(prt_results *r);
@@ -355,7 +364,12 @@ int prt_autotune(const prt_layer *base, const prt_layer *overlay, int op, int64_
 
 /* Intersection area of each pair (subject = base polygon pair_a[i], clip =
  * overlay polygon pair_b[i]) and its gradient with respect to every vertex:
- *   prt_area_fwd: d_area[i] = area(A_i ∩ B_i) (GPC clip + shoelace)
+ *   prt_area_fwd: d_area[i] = area(A_i ∩ B_i), the area of GPC's intersection
+ *                 within 1e-9 relative: the boundary integral over the pieces
+ *                 of each polygon's edges inside the other when every crossing
+ *                 of the pair is clean (the rings of a polygon must not cross
+ *                 each other or themselves; hole rings flagged), else the GPC
+ *                 clip + shoelace of the pair
  *   prt_area_bwd: d_grad_base / d_grad_overlay (V x 2 doubles, accumulated
  *                 with += over pairs; zero them first) += d_upstream[i] *
  *                 d area_i / d vertex, recomputing the boundary pieces. */
@@ -364,6 +378,8 @@ int prt_area_fwd(const int32_t *d_pair_a, const int32_t *d_pair_b, int64_t n_pai
 int prt_area_bwd(const int32_t *d_pair_a, const int32_t *d_pair_b, int64_t n_pairs,
                  const prt_layer *base, const prt_layer *overlay, const double *d_upstream,
                  double *d_grad_base, double *d_grad_overlay, void *stream);
+/* Pairs the last prt_area_fwd call of the process clipped with GPC. */
+int prt_area_fwd_fallbacks(int64_t *h_count);
 
 /* ---------------------------------------------------------------- profiling */
 

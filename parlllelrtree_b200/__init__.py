@@ -273,6 +273,29 @@ class Results:
             out.append([(int(hole[c]), xy[vo[c]:vo[c + 1]]) for c in range(off[i], off[i + 1])])
         return out
 
+    def contours_of(self, pairs) -> list:
+        """Contours of the listed pairs only (prt_results_copy_pairs), as
+        contours() gives them: per pair a list of (hole, [k, 2] vertices)."""
+        idx = np.ascontiguousarray(np.asarray(pairs, dtype=np.int64))
+        k = len(idx)
+        off = np.zeros(k + 1, np.int64)
+        need = np.zeros(2, np.int64)
+        p = lambda a: a.ctypes.data_as(C.c_void_p)
+        cc, vc = 64, 4096
+        while True:
+            nv = np.zeros(cc, np.int32)
+            hole = np.zeros(cc, np.int32)
+            xy = np.zeros((vc, 2), np.float64)
+            rc = lib().prt_results_copy_pairs(self._h, p(idx), k, p(off), p(nv), p(hole), p(xy), cc, vc, p(need))
+            if rc == _lib.PRT_ERR_CAPACITY:
+                cc, vc = max(cc, int(need[0])), max(vc, int(need[1]))
+                continue
+            check(rc)
+            break
+        vo = np.zeros(int(need[0]) + 1, np.int64)
+        np.cumsum(nv[: int(need[0])], out=vo[1:])
+        return [[(int(hole[c]), xy[vo[c]:vo[c + 1]].copy()) for c in range(off[j], off[j + 1])] for j in range(k)]
+
     def area(self) -> torch.Tensor:
         out = torch.empty(self.n_pairs, dtype=torch.float64, device="cuda")
         check(lib().prt_results_area(self._h, _ptr(out), _stream()))

@@ -52,6 +52,7 @@ _SIGS = {
     "prt_results_device": (_I, [_P, _P, _P, _P, _P, _P, _P]),
     "prt_results_copy": (_I, [_P, _P, _P, _P, _P]),
     "prt_results_area": (_I, [_P, _P, _P]),
+    "prt_results_copy_pairs": (_I, [_P, _P, _I64, _P, _P, _P, _P, _I64, _I64, _P]),
     "prt_results_free": (_I, [_P]),
     "prt_clip_pair_host": (_I, [_I, _I, _P, _P, _I, _P, _P, _P, C.c_int32, _P, _P, _P, _I64, _P]),
     "prt_schedule_set": (_I, [_P]),
@@ -67,6 +68,7 @@ _SIGS = {
     "prt_pipeline_free": (_I, [_P]),
     "prt_area_fwd": (_I, [_P, _P, _I64, _P, _P, _P, _P]),
     "prt_area_bwd": (_I, [_P, _P, _I64, _P, _P, _P, _P, _P, _P]),
+    "prt_area_fwd_fallbacks": (_I, [_P]),
     "prt_debug_wait_limit": (_I, [_I, _I]),
     "prt_profile_enable": (_I, [_I]),
     "prt_profile_focus": (_I, [C.c_char_p]),

@@ -1,8 +1,14 @@
 // Intersection area and its adjoint.
 //
-// Forward: area(A_i ∩ B_i) from the GPC clip of each pair (prt_overlay.cu,
-// area-only mode: the clip result is reduced to its shoelace area in place and
-// never written out).
+// Forward: area(A_i ∩ B_i) = the shoelace sum over the boundary of A∩B, i.e.
+// over the pieces of A's edges inside B and of B's edges inside A, found by
+// the same slab / parity pass as the adjoint below (area mode).  Pairs whose
+// crossings are not all clean, whose polygons do not fit the shared-memory
+// staging, or whose area the crossing-rounding bound does not pin to 1e-11 are
+// clipped by GPC instead (prt_overlay.cu, area-only mode: the clip result is
+// reduced to its shoelace area in place and never written out).  The fast
+// path assumes what GPC's output implies for map layers: the rings of a
+// polygon do not cross each other or themselves, and hole rings are flagged.
 //
 // Backward: d area / d vertex by the boundary integral, recomputed from the
 // input polygons rather than stored by the forward pass.  The boundary of
@@ -18,6 +24,8 @@
 // each interval by an even-odd test of its midpoint.  Contributions are scaled by the upstream gradient and
 // accumulated with atomicAdd, since a polygon may appear in many pairs.
 #include <cuda_runtime.h>
+
+#include <atomic>
 
 #include "prt_internal.cuh"
 #include "prt_overlay.cuh"
@@ -424,13 +432,31 @@ __device__ __noinline__ void bwd_edge_exact(const BwdPoly &Q, int nwq, const flo
 // intervals.  The clean path keeps an edge's crossings sorted in registers.
 constexpr int kBwdFast = 4;
 
-__device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int nb, const SlabGrid &g,
-                                const SlabGrid &gx, double w, double *ga, double *gb, int64_t va, int64_t vb,
-                                const Poly &Ag, const Poly &Bg) {
+// Area mode of the same pass (the forward): per edge, the inside length
+// L = sum (t1 - t0) over its inside intervals contributes
+//     s * L * cross(p - O, q - p) / 2
+// to area(A∩B) (the shoelace term of each inside piece, about a pair-local
+// origin O), and every clean crossing adds a bound on how far GPC's own
+// vertex can lie from it: a vertex error of ~eps * max|coordinate| /
+// sin(angle) times the two edges' lengths,
+//     (|r|_1 + |s|_1) * |r|_1 * |s|_1 / |r x s|  (times eps * max|coordinate|).
+struct AreaSum {
+  double area;  // twice the area, summed over the warp by the caller
+  double err;   // the crossing error bound above, without its eps * max|coordinate| factor
+};
+
+// Returns false in area mode as soon as any crossing of the pair is unclean
+// (the caller then clips the pair with GPC); in gradient mode it always runs
+// to the end, by the definition from the first unclean crossing on.
+template <bool kArea>
+__device__ inline bool pair_boundary(const BwdPoly *M, const float4 *ext, int na, int nb, const SlabGrid &g,
+                                     const SlabGrid &gx, double w, double *ga, double *gb, int64_t va, int64_t vb,
+                                     const Poly &Ag, const Poly &Bg, double ox, double oy, AreaSum *acc) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   bool exact = false;  // by the definition from here on (sticky)
   bool carry = false;  // inside state after the last edge of the previous round
+  double area2 = 0.0, err = 0.0;
   for (int e0 = 0; e0 < na + nb; e0 += 32) {
     const int e = e0 + lane;
     const int side = e < na ? 0 : 1;
@@ -483,6 +509,10 @@ __device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int
             unclean = true;
             continue;
           }
+          if constexpr (kArea) {
+            const double sl = fabs(sx) + fabs(sy);
+            err += (rl + sl) * rl * sl / d;
+          }
           double v = (apx * sy - apy * sx) / den;  // next_crossing's t
           // sorted insert into the register list
           if (v < t0c) { const double x = t0c; t0c = v; v = x; }
@@ -495,6 +525,9 @@ __device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int
       unclean |= (m > 1 && t0c == t1c) || (m > 2 && t1c == t2c) || (m > 3 && t2c == t3c);
     }
     exact = __any_sync(kFullMask, unclean) || exact;
+    if constexpr (kArea) {
+      if (exact) return false;
+    }
     double it = 0.0, i1 = 0.0;
     if (exact) {
       if (valid)
@@ -555,6 +588,11 @@ __device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int
         }
       }
     }
+    if constexpr (kArea) {
+      // it + i1 = sum (t1 - t0) over the inside intervals
+      if (valid) area2 += P.sgn[i] * (it + i1) * ((px - ox) * ry - (py - oy) * rx);
+      continue;
+    }
     // contributions: it to the end vertex j, i1 to the start vertex i; the
     // lane of the next edge of the ring hands its start contribution over so
     // the shared vertex takes one atomic per coordinate
@@ -589,6 +627,11 @@ __device__ inline void bwd_pair(const BwdPoly *M, const float4 *ext, int na, int
       atomicAdd(&gr[2 * (vbase + i) + 1], gyi);
     }
   }
+  if constexpr (kArea) {
+    acc->area = area2;
+    acc->err = err;
+  }
+  return true;
 }
 
 // Pairs with a polygon above kBwdMaxV vertices: the global-memory path.
@@ -654,7 +697,8 @@ __global__ void __launch_bounds__(32 * kBwdWarps, 4) area_bwd_kernel(
           bwd_slabs(M, nv, gy, gx);
           Poly A{base.ring_vert, base.ring_hole, base.xy, rr[0], rr[1]};
           Poly B{over.ring_vert, over.ring_hole, over.xy, rr[2], rr[3]};
-          bwd_pair(M, ext, nv[0], nv[1], gy, gx, w, grad_base, grad_over, vb[0], vb[1], A, B);
+          pair_boundary<false>(M, ext, nv[0], nv[1], gy, gx, w, grad_base, grad_over, vb[0], vb[1], A, B, 0.0,
+                               0.0, nullptr);
         }
       } else {
         Poly A{base.ring_vert, base.ring_hole, base.xy, rr[0], rr[1]};
@@ -670,6 +714,110 @@ __global__ void __launch_bounds__(32 * kBwdWarps, 4) area_bwd_kernel(
   }
 }
 
+// Forward: one warp per pair, staged as in the backward.  A pair gets its
+// area from pair_boundary's area mode when every crossing is clean and the
+// crossing error bound stays below kFwdTol of the area; every other pair
+// (polygons above kBwdMaxV vertices or 31 rings, unclean crossings, slivers
+// whose area the bound does not pin to kFwdTol, ids out of range) is listed in
+// fb[] for the GPC clip.  GPC intersects the same edges, so for a clean pair
+// the two areas differ only by the rounding of the crossing vertices, which
+// the bound covers with a factor of 8.
+constexpr double kFwdTol = 1e-11;
+
+// Pairs the last forward call listed for the GPC clip (prt_area_fwd_fallbacks).
+std::atomic<int64_t> g_fwd_fallbacks{0};
+
+__global__ void __launch_bounds__(32 * kBwdWarps, 4) area_fwd_kernel(
+    const int32_t *__restrict__ pa, const int32_t *__restrict__ pb, int64_t n, LayerDev base, LayerDev over,
+    double *__restrict__ area, int32_t *__restrict__ fb, unsigned long long *__restrict__ fb_count) {
+  __shared__ BwdPoly sm[kBwdWarps][2];
+  BwdPoly *M = sm[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  auto fallback = [&](int64_t i) {
+    if (lane == 0) fb[atomicAdd(fb_count, 1ull)] = (int32_t)i;
+  };
+  for (int64_t i = warp; i < n; i += nw) {
+    const int64_t a = pa[i], b = pb[i];
+    if (a < 0 || a >= base.n_poly || b < 0 || b >= over.n_poly) {
+      fallback(i);  // the clip reports the bad id
+      continue;
+    }
+    const int64_t ra0 = base.poly_ring[a], ra1 = base.poly_ring[a + 1];
+    const int64_t rb0 = over.poly_ring[b], rb1 = over.poly_ring[b + 1];
+    int nv[2];
+    int64_t vb[2];
+    float4 ext[2];
+    const bool staged = bwd_load_pair(base, ra0, ra1, over, rb0, rb1, M, nv, vb, ext);
+    if (!staged) {
+      fallback(i);
+      __syncwarp();
+      continue;
+    }
+    const float x0 = fmaxf(ext[0].x, ext[1].x), x1 = fminf(ext[0].z, ext[1].z);
+    const float y0 = fmaxf(ext[0].y, ext[1].y), y1 = fminf(ext[0].w, ext[1].w);
+    if (x0 > x1 || y0 > y1 || nv[0] == 0 || nv[1] == 0) {
+      // boxes apart: no crossing, no point of one inside the other
+      if (lane == 0) area[i] = 0.0;
+      __syncwarp();
+      continue;
+    }
+    const SlabGrid gy = slab_grid(y0, y1), gx = slab_grid(x0, x1);
+    bwd_slabs(M, nv, gy, gx);
+    Poly A{base.ring_vert, base.ring_hole, base.xy, ra0, ra1};
+    Poly B{over.ring_vert, over.ring_hole, over.xy, rb0, rb1};
+    AreaSum acc{0.0, 0.0};
+    const double ox = M[0].x[0], oy = M[0].y[0];  // the pair-local origin
+    const bool ok = pair_boundary<true>(M, ext, nv[0], nv[1], gy, gx, 1.0, nullptr, nullptr, vb[0], vb[1], A, B,
+                                        ox, oy, &acc);
+    if (ok) {
+      double a2 = acc.area, er = acc.err;
+      for (int o = 16; o; o >>= 1) {
+        a2 += __shfl_xor_sync(kFullMask, a2, o);
+        er += __shfl_xor_sync(kFullMask, er, o);
+      }
+      const float cmax = fmaxf(fmaxf(fmaxf(fabsf(ext[0].x), fabsf(ext[0].y)), fmaxf(fabsf(ext[0].z), fabsf(ext[0].w))),
+                               fmaxf(fmaxf(fabsf(ext[1].x), fabsf(ext[1].y)), fmaxf(fabsf(ext[1].z), fabsf(ext[1].w))));
+      const double bound = 8.0 * 2.220446049250313e-16 * (double)cmax * er;
+      const double ar = 0.5 * a2;
+      if (bound <= kFwdTol * fabs(ar)) {
+        if (lane == 0) area[i] = ar;
+      } else {
+        fallback(i);
+      }
+    } else {
+      fallback(i);
+    }
+    __syncwarp();
+  }
+}
+
+__global__ void gather_pairs_kernel(const int32_t *__restrict__ fb, int64_t m, const int32_t *__restrict__ pa,
+                                    const int32_t *__restrict__ pb, int32_t *__restrict__ qa,
+                                    int32_t *__restrict__ qb) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
+    qa[k] = pa[fb[k]];
+    qb[k] = pb[fb[k]];
+  }
+}
+
+__global__ void scatter_area_kernel(const int32_t *__restrict__ fb, int64_t m, const double *__restrict__ src,
+                                    double *__restrict__ area) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x)
+    area[fb[k]] = src[k];
+}
+
+int area_blocks(int64_t n_pairs, const void *kernel) {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, 32 * kBwdWarps, 0) != cudaSuccess || b < 1) {
+    cudaGetLastError();
+    b = 4;
+  }
+  // exactly the resident blocks (each warp loops over pairs): no tail wave
+  return grid_for(n_pairs * 32, 32 * kBwdWarps, b);
+}
+
 }  // namespace
 }  // namespace prt
 
@@ -681,15 +829,68 @@ int prt_area_fwd(const int32_t *d_pair_a, const int32_t *d_pair_b, int64_t n_pai
                  const prt_layer *overlay, double *d_area, void *stream) {
   PRT_CHECK(base && overlay && (n_pairs == 0 || (d_area && d_pair_a && d_pair_b)), PRT_ERR_INVALID,
             "NULL argument");
+  PRT_CHECK(n_pairs >= 0 && n_pairs < (1ll << 31), PRT_ERR_INVALID, "n_pairs=%lld", (long long)n_pairs);
   if (n_pairs == 0) return PRT_OK;
-  PairSrc S;
-  memset(&S, 0, sizeof S);
-  S.pa = d_pair_a;
-  S.pb = d_pair_b;
-  S.base = layer_dev(base);
-  S.over = layer_dev(overlay);
-  S.op = PRT_GPC_INT;
-  return overlay_impl(S, n_pairs, PRT_SCHED_BATCHED, d_area, reinterpret_cast<cudaStream_t>(stream), nullptr);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  // boundary integral for the clean pairs, the list of the others
+  unsigned char *scr = nullptr;
+  int rc = dmalloc(reinterpret_cast<void **>(&scr), 64 + 4 * (size_t)n_pairs, s);
+  if (rc) return rc;
+  unsigned long long *cnt = reinterpret_cast<unsigned long long *>(scr);
+  int32_t *fb = reinterpret_cast<int32_t *>(scr + 64);
+  cudaError_t e = cudaMemsetAsync(cnt, 0, 8, s);
+  if (e == cudaSuccess) {
+    PRT_PROF("area_fwd", s);
+    area_fwd_kernel<<<area_blocks(n_pairs, (const void *)area_fwd_kernel), 32 * kBwdWarps, 0, s>>>(
+      d_pair_a, d_pair_b, n_pairs, layer_dev(base), layer_dev(overlay), d_area, fb, cnt);
+    e = cudaGetLastError();
+  }
+  unsigned long long m = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&m, cnt, 8, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    dfree(scr, s);
+    return cuda_status(e, "area forward");
+  }
+  g_fwd_fallbacks.store((int64_t)m);
+  if (m > 0) {
+    // the listed pairs: GPC clip, area of its result (area-only mode)
+    int32_t *q = nullptr;
+    double *ar = nullptr;
+    rc = dalloc(&q, 2 * m, s);
+    if (!rc) rc = dalloc(&ar, m, s);
+    if (!rc) {
+      {
+        PRT_PROF("gather_pairs", s);
+        gather_pairs_kernel<<<grid_for((int64_t)m, 256, 8), 256, 0, s>>>(fb, (int64_t)m, d_pair_a, d_pair_b, q,
+                                                                           q + m);
+      }
+      PairSrc S;
+      memset(&S, 0, sizeof S);
+      S.pa = q;
+      S.pb = q + m;
+      S.base = layer_dev(base);
+      S.over = layer_dev(overlay);
+      S.op = PRT_GPC_INT;
+      rc = overlay_impl(S, (int64_t)m, PRT_SCHED_BATCHED, ar, s, nullptr);
+    }
+    if (!rc) {
+      PRT_PROF("scatter_area", s);
+      scatter_area_kernel<<<grid_for((int64_t)m, 256, 8), 256, 0, s>>>(fb, (int64_t)m, ar, d_area);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) rc = cuda_status(e, "area scatter");
+    }
+    dfree(q, s);
+    dfree(ar, s);
+  }
+  dfree(scr, s);
+  return rc;
+}
+
+int prt_area_fwd_fallbacks(int64_t *h_count) {
+  PRT_CHECK(h_count, PRT_ERR_INVALID, "NULL argument");
+  *h_count = g_fwd_fallbacks.load();
+  return PRT_OK;
 }
 
 int prt_area_bwd(const int32_t *d_pair_a, const int32_t *d_pair_b, int64_t n_pairs, const prt_layer *base,
@@ -701,15 +902,7 @@ int prt_area_bwd(const int32_t *d_pair_a, const int32_t *d_pair_b, int64_t n_pai
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   {
     PRT_PROF("area_bwd", s);
-    // exactly the resident blocks (each warp loops over pairs): no tail wave
-    static int per_sm = 0;
-    if (per_sm == 0) {
-      int b = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, area_bwd_kernel, 32 * kBwdWarps, 0) != cudaSuccess || b < 1)
-        b = 4;
-      per_sm = b;
-    }
-    const int blocks = grid_for(n_pairs * 32, 32 * kBwdWarps, per_sm);
+    const int blocks = area_blocks(n_pairs, (const void *)area_bwd_kernel);
     area_bwd_kernel<<<blocks, 32 * kBwdWarps, 0, s>>>(d_pair_a, d_pair_b, n_pairs, layer_dev(base),
                                                       layer_dev(overlay), d_upstream, d_grad_base, d_grad_overlay);
   }

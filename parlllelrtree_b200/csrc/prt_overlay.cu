@@ -1140,6 +1140,57 @@ int prt_results_copy(const prt_results *r, int64_t *h_pair_cont_off, int32_t *h_
   return PRT_OK;
 }
 
+int prt_results_copy_pairs(const prt_results *r, const int64_t *h_pairs, int64_t k, int64_t *h_pair_cont_off,
+                           int32_t *h_cont_nverts, int32_t *h_cont_hole, double *h_xy, int64_t cont_cap,
+                           int64_t vert_cap, int64_t *h_need) {
+  PRT_CHECK(r && (k == 0 || h_pairs) && h_pair_cont_off && h_need, PRT_ERR_INVALID, "NULL argument");
+  PRT_CHECK(k >= 0, PRT_ERR_INVALID, "k < 0");
+  for (int64_t j = 0; j < k; j++)
+    PRT_CHECK(h_pairs[j] >= 0 && h_pairs[j] < r->n_pairs, PRT_ERR_INVALID, "pair %lld out of range",
+              (long long)h_pairs[j]);
+  PRT_CUDA(cudaDeviceSynchronize());
+  std::vector<int64_t> cs(k);
+  std::vector<int32_t> nc(k);
+  for (int64_t j = 0; j < k; j++) {
+    PRT_CUDA(cudaMemcpy(&cs[j], r->pair_cstart + h_pairs[j], 8, cudaMemcpyDeviceToHost));
+    PRT_CUDA(cudaMemcpy(&nc[j], r->pair_ncont + h_pairs[j], 4, cudaMemcpyDeviceToHost));
+  }
+  // contour headers of the listed pairs, then their vertices
+  std::vector<int64_t> cvs;
+  std::vector<int32_t> cnv, ch;
+  h_pair_cont_off[0] = 0;
+  for (int64_t j = 0; j < k; j++) {
+    const size_t o = cvs.size();
+    cvs.resize(o + nc[j]);
+    cnv.resize(o + nc[j]);
+    ch.resize(o + nc[j]);
+    if (nc[j]) {
+      PRT_CUDA(cudaMemcpy(cvs.data() + o, r->cont_vstart + cs[j], 8 * (size_t)nc[j], cudaMemcpyDeviceToHost));
+      PRT_CUDA(cudaMemcpy(cnv.data() + o, r->cont_nverts + cs[j], 4 * (size_t)nc[j], cudaMemcpyDeviceToHost));
+      PRT_CUDA(cudaMemcpy(ch.data() + o, r->cont_hole + cs[j], 4 * (size_t)nc[j], cudaMemcpyDeviceToHost));
+    }
+    h_pair_cont_off[j + 1] = (int64_t)cvs.size();
+  }
+  int64_t nv = 0;
+  for (int32_t v : cnv) nv += v;
+  h_need[0] = (int64_t)cvs.size();
+  h_need[1] = nv;
+  if (h_need[0] > cont_cap || nv > vert_cap) {
+    set_error("results_copy_pairs: %lld contours / %lld vertices exceed the buffers", (long long)h_need[0],
+              (long long)nv);
+    return PRT_ERR_CAPACITY;
+  }
+  PRT_CHECK(cvs.empty() || (h_cont_nverts && h_cont_hole && h_xy), PRT_ERR_INVALID, "NULL argument");
+  int64_t v = 0;
+  for (size_t c = 0; c < cvs.size(); c++) {
+    h_cont_nverts[c] = cnv[c];
+    h_cont_hole[c] = ch[c];
+    if (cnv[c]) PRT_CUDA(cudaMemcpy(h_xy + 2 * v, r->xy + 2 * cvs[c], 16 * (size_t)cnv[c], cudaMemcpyDeviceToHost));
+    v += cnv[c];
+  }
+  return PRT_OK;
+}
+
 int prt_results_area(const prt_results *r, double *d_area, void *stream) {
   PRT_CHECK(r && d_area, PRT_ERR_INVALID, "NULL argument");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

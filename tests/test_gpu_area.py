@@ -137,3 +137,76 @@ def test_shared_polygons_accumulate(cuda):
     v0 = slice(A["ring_vert"][0], A["ring_vert"][1])
     ref = 2 * g00 + g01
     assert np.abs(g[v0] - ref).max() <= 1e-9 * np.abs(ref).max() + 1e-20
+
+
+def _degenerate_pairs():
+    """Pairs where the boundary integral's crossings are not clean or the
+    area is a sliver: identical polygons, a shared edge, a vertex on an edge,
+    one polygon inside the other, disjoint polygons with overlapping boxes,
+    a thin sliver, and a square against a square with a square hole."""
+    sq = lambda x0, y0, s: np.array([[x0, y0], [x0 + s, y0], [x0 + s, y0 + s], [x0, y0 + s]], np.float64)
+    tri = np.array([[0.5, 0.5], [0.52, 0.5], [0.51, 0.52]])
+    ring_a, ring_b, hole_a, hole_b, rpa, rpb = [], [], [], [], [], []
+
+    def add(a_rings, b_rings, a_holes=None, b_holes=None):
+        ring_a.extend(a_rings)
+        ring_b.extend(b_rings)
+        hole_a.extend(a_holes or [0] * len(a_rings))
+        hole_b.extend(b_holes or [0] * len(b_rings))
+        rpa.append(len(a_rings))
+        rpb.append(len(b_rings))
+
+    s0 = sq(0.3, 0.3, 0.01)
+    add([s0], [s0.copy()])                                          # identical
+    add([s0], [sq(0.31, 0.3, 0.01)])                                # shared edge
+    add([s0], [np.array([[0.305, 0.31], [0.32, 0.315], [0.31, 0.33]])])  # vertex on an edge
+    add([s0], [sq(0.302, 0.302, 0.004)])                            # nested, no crossing
+    add([tri], [np.array([[0.52, 0.505], [0.53, 0.505], [0.53, 0.52]])])  # boxes overlap, disjoint
+    add([sq(0.4, 0.4, 0.01)], [sq(0.4 + 0.01 - 1e-13, 0.403, 0.01)])      # sliver 1e-13 wide
+    add([sq(0.6, 0.6, 0.02)], [sq(0.605, 0.605, 0.02), sq(0.61, 0.61, 0.005)[::-1]], None, [0, 1])  # hole
+    add([sq(0.7, 0.7, 0.01)], [sq(0.705, 0.695, 0.01)])             # two clean crossings
+    A = dg.layer_from_rings(ring_a, hole_a, rpa)
+    B = dg.layer_from_rings(ring_b, hole_b, rpb)
+    return A, B
+
+
+def test_forward_falls_back_to_gpc_on_degenerate_pairs(cuda):
+    import parlllelrtree_b200 as prt
+    from parlllelrtree_b200 import _lib
+
+    A, B = _degenerate_pairs()
+    n = len(A["poly_ring"]) - 1
+    LA, LB = prt.Layer.from_dict(A), prt.Layer.from_dict(B)
+    idx = torch.arange(n, dtype=torch.int32, device="cuda")
+    area = prt.intersection_area(LA, LB, idx, idx).cpu().numpy()
+    for i in range(n):
+        ref = oracle.result_area(oracle.gpc_clip(rings_of(A, i), rings_of(B, i), 1))
+        assert abs(area[i] - ref) <= 1e-9 * abs(ref) + 1e-22, (i, area[i], ref)
+    fb = __import__("ctypes").c_int64(-1)
+    _lib.check(_lib.lib().prt_area_fwd_fallbacks(__import__("ctypes").byref(fb)))
+    # identical, shared edge, vertex on edge, sliver at least go to GPC
+    assert fb.value >= 4
+
+
+def test_forward_differentiable_configuration(cuda):
+    """The differentiable-area configuration's pairs (16-64 vertices, overlap
+    guaranteed): the device forward against the oracle's GPC area on 20,000
+    pairs, and most pairs on the boundary-integral path."""
+    import ctypes
+
+    import parlllelrtree_b200 as prt
+    from parlllelrtree_b200 import _lib
+
+    n = 20000
+    Ad, Bd = dg.overlapping_pairs_device(n, seed=5)
+    LA, LB = prt.Layer.from_dict(Ad), prt.Layer.from_dict(Bd)
+    idx = torch.arange(n, dtype=torch.int32, device="cuda")
+    area = prt.intersection_area(LA, LB, idx, idx).cpu().numpy()
+    fb = ctypes.c_int64(-1)
+    _lib.check(_lib.lib().prt_area_fwd_fallbacks(ctypes.byref(fb)))
+    assert fb.value < 0.05 * n
+    A = {k: v.cpu().numpy() for k, v in Ad.items()}
+    B = {k: v.cpu().numpy() for k, v in Bd.items()}
+    for i in range(n):
+        ref = oracle.result_area(oracle.gpc_clip(rings_of(A, i), rings_of(B, i), 1))
+        assert abs(area[i] - ref) <= 1e-9 * abs(ref) + 1e-22, (i, area[i], ref)
