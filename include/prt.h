@@ -245,6 +245,23 @@ int prt_results_copy_pairs(const prt_results *r, const int64_t *h_pairs, int64_t
 int prt_results_area(const prt_results *r, double *d_area, void *stream);
 int prt_results_free(prt_results *r);
 
+/* Streaming overlay (no reference counterpart; the reference's results live
+ * in a 1 GiB device heap, vector_map_overlay_gpc_kernel.cu:72): the pairs of
+ * prt_overlay_run are clipped in chunks of at most chunk_pairs, and each
+ * chunk's results are copied to pinned host memory in pair order and passed
+ * to fn before their device memory is released, so device memory holds at
+ * most two chunks' results however large the whole result set is.  A chunk's
+ * copy-out overlaps the next chunk's clip.  fn receives the chunk's first
+ * pair index and pair count and, valid only during the call, the CSR of
+ * prt_results_copy (pair_cont_off [n+1] relative to the chunk, cont_nverts /
+ * cont_hole per contour, xy as x, y pairs); a non-zero return stops the
+ * stream (PRT_ERR_INVALID). */
+typedef int (*prt_chunk_fn)(void *user, int64_t first_pair, int64_t n_pairs, const int64_t *pair_cont_off,
+                            const int32_t *cont_nverts, const int32_t *cont_hole, const double *xy);
+int prt_overlay_stream(const prt_pair *d_pairs, int64_t n_pairs, int32_t offset,
+                       const int32_t *d_leaf_to_poly, const prt_layer *base, const prt_layer *overlay,
+                       int op, int sched, int64_t chunk_pairs, prt_chunk_fn fn, void *user, void *stream);
+
 /* One pair from host memory (rings as counts + packed xy), clipped on the
  * device; the result is written to host buffers.  Returns PRT_ERR_CAPACITY
  * (with *out_ncont / *out_nv set) when cont_cap / vert_cap are too small. */
@@ -393,6 +410,35 @@ int prt_profile_enable(int mode);
 int prt_profile_focus(const char *kernel_name);
 int prt_profile_reset(void);
 int prt_profile_read(char *names, int names_cap, double *ms_total, int64_t *launches, int cap);
+
+/* ---------------------------------------------------------------- text files */
+
+/* The reference's input files (host code; no device needed).
+ * Rect file, data/Rect1024.txt of the R-tree programs (BotomUp-rtree.cu:669-698,
+ * TopDown-rtree.cu:487-497): the record count, then per record "x1 x2",
+ * "y1 y2" (integers) and an integer key.  Boxes are returned / taken as
+ * n x 4 int64 (x1, y1, x2, y2); keys as int32 (NULL when writing: 0..n-1).
+ * A count above cap returns PRT_ERR_CAPACITY with *n_read set. */
+int prt_rect_file_count(const char *path, int64_t *n);
+int prt_read_rect_file(const char *path, int64_t *h_boxes, int32_t *h_keys, int64_t cap, int64_t *n_read);
+int prt_write_rect_file(const char *path, const int64_t *h_boxes, const int32_t *h_keys, int64_t n);
+
+/* Polygon file, the base / overlay files of readData
+ * (vector_map_overlay_gpc_kernel.cu:752-888): the polygon count, then per
+ * polygon its vertex count, hole flag, bounding box (four doubles x1 y1 x2 y2)
+ * and vertices ("x y" pairs).  prt_read_polygon_file fills readData's arrays:
+ * num[], prefix[] (int64, prefix[i] = prefix[i-1] + num[i-1]), hole[], the box
+ * as read (h_mbr, n x 4, optional), the box quantised as readData does
+ * ((int)(v * 100000), h_rect, n x 4, optional) and the vertices (x, y pairs,
+ * optional).  prt_polygon_file_size gives the counts to size them; caps that
+ * are too small return PRT_ERR_CAPACITY.  prt_write_polygon_file writes the
+ * exact vertex bounds as the box, every double in a form that reads back to
+ * the same value (%.17g). */
+int prt_polygon_file_size(const char *path, int64_t *n_poly, int64_t *n_vert);
+int prt_read_polygon_file(const char *path, int32_t *h_num, int64_t *h_prefix, int32_t *h_hole, double *h_mbr,
+                          int32_t *h_rect, double *h_vertex, int64_t poly_cap, int64_t vert_cap);
+int prt_write_polygon_file(const char *path, const int32_t *h_num, const int32_t *h_hole, const double *h_vertex,
+                           int64_t n_poly);
 
 /* ---------------------------------------------------------------- bounded waits */
 

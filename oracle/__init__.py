@@ -349,6 +349,37 @@ def ref_overlap(a, b, which: str = "bu") -> int:
     return int(ref_lib("libref_td_m10.so").ref_td_overlap(_p(a), _p(b)))
 
 
+def ref_read_data(base: str, overlay: str, min_xy=(2**31 - 1, 2**31 - 1)) -> dict:
+    """The reference's own readData (vector_map_overlay_gpc_kernel.cu:752-888,
+    host build in oracle/_ref/libref_readdata.so) on two polygon files:
+    {"base": {...}, "overlay": {...}, "min_xy": (minX, minY)} with num, prefix,
+    hole, rect (P x 4, its quantised boxes) and vertex (V x 2) per layer."""
+    L = ref_lib("libref_readdata.so")
+    counts = np.zeros(4, np.int64)
+    mxy = np.array(min_xy, np.int32)
+    cap_p = cap_v = 0
+    while True:
+        bufs = [{"num": np.zeros(max(cap_p, 1), np.int32), "prefix": np.zeros(max(cap_p, 1), np.int64),
+                 "hole": np.zeros(max(cap_p, 1), np.int32), "rect": np.zeros((max(cap_p, 1), 4), np.int32),
+                 "vertex": np.zeros((max(cap_v, 1), 2), np.float64)} for _ in range(2)]
+        m = mxy.copy()
+        args = [base.encode(), overlay.encode(), _p(counts)]
+        for b in bufs:
+            args += [_p(b["num"]), _p(b["prefix"]), _p(b["hole"]), _p(b["rect"]), _p(b["vertex"])]
+        args += [C.c_int64(cap_p), C.c_int64(cap_v), _p(m)]
+        rc = L.ref_read_data(*args)
+        if rc == 0:
+            break
+        cap_p, cap_v = int(max(counts[0], counts[1])), int(max(counts[2], counts[3]))
+    out = {}
+    for k, (name, b) in enumerate(zip(("base", "overlay"), bufs)):
+        P, V = int(counts[k]), int(counts[2 + k])
+        out[name] = {"num": b["num"][:P], "prefix": b["prefix"][:P], "hole": b["hole"][:P], "rect": b["rect"][:P],
+                     "vertex": b["vertex"][:V]}
+    out["min_xy"] = (int(m[0]), int(m[1]))
+    return out
+
+
 def write_rect_file(path: str, rects: np.ndarray, keys=None) -> None:
     """Writes boxes in the format TopDown-rtree.cu / BotomUp-rtree.cu read
     (N, then per box "x1 x2", "y1 y2", "key"; BU:671-698, TD:487-497)."""

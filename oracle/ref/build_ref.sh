@@ -17,6 +17,9 @@
 #                        RtreeSearch1 (TD:56-93), at fanout M = F.
 #   libref_gpc.so        Host build of the reference's GPC clip core
 #                        (vector_map_overlay_gpc_kernel.cu:115-750, 890-1709).
+#   libref_readdata.so   Host build of readData, the polygon file reader
+#                        (vector_map_overlay_gpc_kernel.cu:752-888), with its
+#                        cudaMalloc / cudaMemcpy as host allocations and copies.
 #
 # The reference files are read where they lie; the line ranges below are
 # extracted into oracle/_ref/*.slice.inc (build intermediates, never committed)
@@ -94,6 +97,12 @@ done
   slice "$GPC" 890 1709 "__device__ void gpc_free_polygon"
 } > "$OUT/gpc_core.slice.inc"
 g++ $CXXFLAGS -I"$HERE" -I"$OUT" -o "$OUT/libref_gpc.so" "$HERE/gpc_ref_harness.cpp"
+
+# ---- readData (the polygon file reader) ------------------------------------------
+{
+  slice "$GPC" 752 888 "void readData(char * base_filename"
+} > "$OUT/readdata.slice.inc"
+g++ $CXXFLAGS -I"$HERE" -I"$OUT" -o "$OUT/libref_readdata.so" "$HERE/readdata_harness.cpp"
 
 # ---- TD program, unchanged -------------------------------------------------------
 if command -v nvcc >/dev/null 2>&1; then

@@ -30,7 +30,7 @@ from ._lib import COORD, KEY, OP, SCHED, PrtError, check, lib
 __all__ = [
     "Tree", "Layer", "Results", "build_bottomup", "build_topdown", "overlay", "overlay_ref", "clip_pair",
     "intersection_area", "IntersectionArea", "PrtError", "device_count", "Pipeline", "get_schedule",
-    "set_schedule", "schedule", "autotune",
+    "set_schedule", "schedule", "autotune", "overlay_stream",
 ]
 
 _DT2COORD = {torch.int64: COORD["i64"], torch.float32: COORD["f32"], torch.float64: COORD["f64"],
@@ -313,6 +313,43 @@ def overlay(pairs, base: Layer, over: Layer, leaf_to_poly=None, offset: int = 0,
     check(lib().prt_overlay_run(_ptr(p), len(p), offset, _ptr(l2p), C.byref(sb), C.byref(so), OP[op], SCHED[sched],
                                 _stream(), C.byref(h)))
     return Results(h)
+
+
+_CHUNK_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                       C.POINTER(C.c_int32), C.POINTER(C.c_double))
+
+
+def overlay_stream(pairs, base: Layer, over: Layer, fn, leaf_to_poly=None, offset: int = 0, op: str = "int",
+                   sched: str = "batched", chunk_pairs: int = 1 << 18) -> None:
+    """Clips the pairs in chunks of at most ``chunk_pairs`` (prt_overlay_stream):
+    device memory holds at most two chunks' results.  For every chunk, in pair
+    order, ``fn(first_pair, pair_cont_off, cont_nverts, cont_hole, xy)`` gets
+    numpy copies of its results (pair_cont_off relative to the chunk, xy
+    [V, 2]); a truthy return value stops the stream with an error."""
+    p = _dev_tensor(pairs, torch.int32)
+    l2p = _dev_tensor(leaf_to_poly, torch.int32) if leaf_to_poly is not None else None
+    sb, so = base.struct(), over.struct()
+    err = []
+
+    def cb(user, first, n, off, nv, hole, xy):
+        try:
+            o = np.ctypeslib.as_array(off, shape=(n + 1,)).copy()
+            nc = int(o[-1])
+            nvv = np.ctypeslib.as_array(nv, shape=(max(nc, 1),))[:nc].copy()
+            hh = np.ctypeslib.as_array(hole, shape=(max(nc, 1),))[:nc].copy()
+            tv = int(nvv.sum())
+            xx = np.ctypeslib.as_array(xy, shape=(max(tv, 1), 2))[:tv].copy()
+            return 1 if fn(int(first), o, nvv, hh, xx) else 0
+        except BaseException as e:  # surfaced after the C call returns
+            err.append(e)
+            return 1
+
+    cfn = _CHUNK_FN(cb)
+    rc = lib().prt_overlay_stream(_ptr(p), len(p), offset, _ptr(l2p), C.byref(sb), C.byref(so), OP[op], SCHED[sched],
+                                  int(chunk_pairs), C.cast(cfn, C.c_void_p), None, _stream())
+    if err:
+        raise err[0]
+    check(rc)
 
 
 MAX_BINS = 8

@@ -70,6 +70,13 @@ _SIGS = {
     "prt_area_bwd": (_I, [_P, _P, _I64, _P, _P, _P, _P, _P, _P]),
     "prt_area_fwd_fallbacks": (_I, [_P]),
     "prt_debug_wait_limit": (_I, [_I, _I]),
+    "prt_overlay_stream": (_I, [_P, _I64, C.c_int32, _P, _P, _P, _I, _I, _I64, _P, _P, _P]),
+    "prt_rect_file_count": (_I, [C.c_char_p, _P]),
+    "prt_read_rect_file": (_I, [C.c_char_p, _P, _P, _I64, _P]),
+    "prt_write_rect_file": (_I, [C.c_char_p, _P, _P, _I64]),
+    "prt_polygon_file_size": (_I, [C.c_char_p, _P, _P]),
+    "prt_read_polygon_file": (_I, [C.c_char_p, _P, _P, _P, _P, _P, _P, _I64, _I64]),
+    "prt_write_polygon_file": (_I, [C.c_char_p, _P, _P, _P, _I64]),
     "prt_profile_enable": (_I, [_I]),
     "prt_profile_focus": (_I, [C.c_char_p]),
     "prt_profile_reset": (_I, []),

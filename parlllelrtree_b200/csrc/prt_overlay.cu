@@ -841,18 +841,6 @@ int overlay_graph_enqueue(const PairSrc &S, const unsigned long long *d_npairs, 
 
 }  // namespace prt
 
-struct prt_results {
-  int64_t n_pairs, n_cont, n_vert, nonempty, retried;
-  int64_t *pair_cstart;
-  int32_t *pair_ncont;
-  int32_t *status;
-  int64_t *cont_vstart;
-  int32_t *cont_nverts;
-  int32_t *cont_hole;
-  double *xy;
-  unsigned long long *pool;
-};
-
 namespace prt {
 
 static void free_state(OverlayState &st, cudaStream_t s) {

@@ -118,3 +118,19 @@ struct GraphOverlay {
 int overlay_graph_enqueue(const PairSrc &S, const unsigned long long *d_npairs, GraphOverlay &G, cudaStream_t s);
 
 }  // namespace prt
+
+// A result set (the reference's per-pair gpc_polygon array): pair i owns
+// contours [pair_cstart[i], + pair_ncont[i]) of the pools, contour c owns
+// vertices [cont_vstart[c], + cont_nverts[c]) of xy.  Pools are filled by
+// atomic reservations, so they are not in pair order.
+struct prt_results {
+  int64_t n_pairs, n_cont, n_vert, nonempty, retried;
+  int64_t *pair_cstart;
+  int32_t *pair_ncont;
+  int32_t *status;
+  int64_t *cont_vstart;
+  int32_t *cont_nverts;
+  int32_t *cont_hole;
+  double *xy;
+  unsigned long long *pool;
+};
