@@ -23,7 +23,13 @@ namespace {
 constexpr int kRadix = 256;
 constexpr int kSortBlock = 256;
 constexpr int kSortWarps = kSortBlock / 32;
-constexpr int kItems = 12;
+#ifndef PRT_SORT_ITEMS
+#define PRT_SORT_ITEMS 12  // keys per thread of a tile
+#endif
+#ifndef PRT_SORT_MIN_BLOCKS
+#define PRT_SORT_MIN_BLOCKS 4  // resident blocks per SM the pass is compiled for
+#endif
+constexpr int kItems = PRT_SORT_ITEMS;
 constexpr int kTile = kSortBlock * kItems;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
@@ -115,10 +121,16 @@ struct PassSmem {
   int tile;
 };
 
-constexpr int kLookBatch = 16;  // predecessor statuses read per look-back step
+#ifndef PRT_SORT_LOOKBATCH
+#define PRT_SORT_LOOKBATCH 16
+#endif
+#ifndef PRT_SORT_BACKOFF_NS
+#define PRT_SORT_BACKOFF_NS 0  // pause between look-back polls that found nothing new
+#endif
+constexpr int kLookBatch = PRT_SORT_LOOKBATCH;  // predecessor statuses read per look-back step
 
 template <typename KeyT>
-__global__ void __launch_bounds__(kSortBlock, 4) onesweep_pass(KeyT *keys0, uint32_t *vals0, KeyT *keys1,
+__global__ void __launch_bounds__(kSortBlock, PRT_SORT_MIN_BLOCKS) onesweep_pass(KeyT *keys0, uint32_t *vals0, KeyT *keys1,
                                                            uint32_t *vals1, int64_t n, int shift,
                                                            const PassPlan *__restrict__ plan,
                                                            const uint32_t *__restrict__ goff,
@@ -263,9 +275,12 @@ __global__ void __launch_bounds__(kSortBlock, 4) onesweep_pass(KeyT *keys0, uint
       }
       if (done) break;
       t -= used;
-      if (used == 0 && ++spins > wl.polls) {
-        timed_out = true;
-        break;
+      if (used == 0) {
+        if (++spins > wl.polls) {
+          timed_out = true;
+          break;
+        }
+        if (PRT_SORT_BACKOFF_NS > 0) __nanosleep(PRT_SORT_BACKOFF_NS);
       }
     }
     if (timed_out) atomicOr(err, kErrTimeout);
