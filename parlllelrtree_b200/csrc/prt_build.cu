@@ -345,43 +345,213 @@ __global__ void select_copy_u32_kernel(const uint32_t *a, const uint32_t *b, con
     dst[i] = src[i];
 }
 
+// ------------------------------------------------------------------ top-down, short runs
+
+// A top-down level whose runs hold at most kTdLocal records is sorted run by
+// run in shared memory: one CTA takes as many whole runs as fit in a tile of
+// kTdLocal records (in the current order), gathers each record's coordinate
+// key, and sorts the tile stably by (run within the tile, key) with an LSD
+// radix sort in shared memory, 8 bits per pass, each pass ranked by the warp
+// multisplit (lanes with the same digit from one ballot per digit bit).  The
+// tile's index order is the current order, so equal keys keep it, as the
+// level's stable sort requires.  This replaces 4-7 global passes over 64-bit
+// keys by one gather, one read and one write of the order.
+constexpr int kTdLocal = 4096;
+constexpr int kTdItems = kTdLocal / 256;  // per thread (256 threads)
+
+__device__ __forceinline__ uint32_t lane_lt() {
+  uint32_t m;
+  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <typename K>
+struct TdLocalSmem {
+  K key[2][kTdLocal];
+  uint32_t val[2][kTdLocal];
+  uint32_t wh[8][256];
+  uint32_t dstart[256];
+  uint32_t wsum[8];
+};
+
+template <typename T, typename K>
+__global__ void __launch_bounds__(256) td_local_sort_kernel(const Box<T> *__restrict__ b,
+                                                            const uint32_t *__restrict__ perm_in, int64_t n,
+                                                            int64_t seg, int use_y, int run_bits,
+                                                            uint32_t *__restrict__ perm_out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TdLocalSmem<K> &S = *reinterpret_cast<TdLocalSmem<K> *>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t chunk = (kTdLocal / seg) * seg;  // whole runs per tile
+  const int64_t base = blockIdx.x * chunk;
+  const int m = (int)min(chunk, n - base);
+  constexpr int kKeyBits = 8 * (int)sizeof(K);
+  const T *c = reinterpret_cast<const T *>(b);
+  // keys: (run within the tile) above the coordinate's order-preserving image
+  for (int i = tid; i < m; i += 256) {
+    uint32_t r = perm_in ? perm_in[base + i] : (uint32_t)(base + i);
+    if ((int64_t)r >= n) r = 0;  // only after a timed-out sort (reported by the caller)
+    const T v = __ldg(&c[4 * (int64_t)r + (use_y ? 1 : 0)]);
+    S.key[0][i] = (K)ukey(v);
+    S.val[0][i] = r;
+  }
+  __syncthreads();
+  const int total_bits = kKeyBits + run_bits;
+  const uint32_t lt = lane_lt();
+  int cur = 0;
+  for (int shift = 0; shift < total_bits; shift += 8) {
+    for (int i = tid; i < 8 * 256; i += 256) (&S.wh[0][0])[i] = 0;
+    __syncthreads();
+    // digit of item i: the key's byte, or above the key the run index
+    auto digit = [&](int i) -> int {
+      if (shift < kKeyBits) return (int)((S.key[cur][i] >> shift) & 0xFF);
+      return (int)(((int64_t)i / seg >> (shift - kKeyBits)) & 0xFF);
+    };
+    int dg[kTdItems];
+    uint32_t rk[kTdItems];
+    uint32_t *wh = S.wh[warp];
+#pragma unroll
+    for (int j = 0; j < kTdItems; j++) {
+      const int i = warp * (32 * kTdItems) + j * 32 + lane;
+      const bool ok = i < m;
+      const int d = ok ? digit(i) : 256 + lane;
+      uint32_t peers = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+      for (int bit = 0; bit < 8; bit++) {
+        const uint32_t bm = __ballot_sync(0xffffffffu, (d >> bit) & 1);
+        peers &= ((d >> bit) & 1) ? bm : ~bm;
+      }
+      if (!ok) peers = 1u << lane;
+      const int leader = __ffs(peers) - 1;
+      uint32_t cnt = 0;
+      if (lane == leader && ok) {
+        cnt = wh[d];
+        wh[d] = cnt + __popc(peers);
+      }
+      cnt = __shfl_sync(0xffffffffu, cnt, leader);
+      dg[j] = d;
+      rk[j] = cnt + __popc(peers & lt);
+      __syncwarp();
+    }
+    __syncthreads();
+    // thread d: exclusive prefix of digit d over the warps, then over digits
+    uint32_t tot = 0;
+#pragma unroll
+    for (int w = 0; w < 8; w++) {
+      const uint32_t x = S.wh[w][tid];
+      S.wh[w][tid] = tot;
+      tot += x;
+    }
+    uint32_t incl = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) S.wsum[warp] = incl;
+    __syncthreads();
+    uint32_t woff = 0;
+#pragma unroll
+    for (int w = 0; w < 8; w++) woff += w < warp ? S.wsum[w] : 0u;
+    S.dstart[tid] = woff + incl - tot;
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kTdItems; j++) {
+      const int i = warp * (32 * kTdItems) + j * 32 + lane;
+      if (i < m) {
+        const uint32_t pos = S.dstart[dg[j]] + S.wh[warp][dg[j]] + rk[j];
+        S.key[1 - cur][pos] = S.key[cur][i];
+        S.val[1 - cur][pos] = S.val[cur][i];
+      }
+    }
+    cur = 1 - cur;
+    __syncthreads();
+  }
+  for (int i = tid; i < m; i += 256) perm_out[base + i] = S.val[cur][i];
+}
+
+// Launches the short-run sort of one top-down level (seg <= kTdLocal).
+template <typename T>
+int td_local_level(const void *d_boxes, const uint32_t *perm_in, int64_t n, int64_t seg, int use_y,
+                   uint32_t *perm_out, cudaStream_t s) {
+  using K = typename std::conditional<sizeof(T) == 8, uint64_t, uint32_t>::type;
+  const int64_t chunk = (kTdLocal / seg) * seg;
+  int run_bits = 0;
+  while ((1ll << run_bits) < kTdLocal / seg) run_bits++;
+  const size_t smem = sizeof(TdLocalSmem<K>);
+  static bool attr_done[256] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 256 || !attr_done[dev]) {
+    PRT_CUDA(cudaFuncSetAttribute(td_local_sort_kernel<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    if (dev >= 0 && dev < 256) attr_done[dev] = true;
+  }
+  const int64_t blocks = (n + chunk - 1) / chunk;
+  {
+    PRT_PROF("td_local_sort", s);
+    td_local_sort_kernel<T, K><<<(unsigned)blocks, 256, smem, s>>>(reinterpret_cast<const Box<T> *>(d_boxes),
+                                                                   perm_in, n, seg, use_y, run_bits, perm_out);
+  }
+  PRT_CUDA(cudaGetLastError());
+  return PRT_OK;
+}
+
 // ------------------------------------------------------------------ packing
 
 // Leaf level: gather the records in leaf order (coalesced writes), their ids,
-// and when F divides 32, the leaf-node unions for level 1 by shuffles.
+// and when F divides 32, the leaf-node unions for level 1 by shuffles.  The
+// gather by sort index is random, so each warp takes kLeafUnroll chunks of 32
+// consecutive leaves at a time and issues all their index loads, then all
+// their box loads, before using any: more independent loads in flight.
+constexpr int kLeafUnroll = 4;
+
 template <typename T, int F>
-__global__ void pack_leaf_kernel(const Box<T> *__restrict__ b, const int32_t *__restrict__ ids,
+__global__ void __launch_bounds__(256) pack_leaf_kernel(const Box<T> *__restrict__ b, const int32_t *__restrict__ ids,
                                  const uint32_t *__restrict__ perm_a, const uint32_t *__restrict__ perm_b,
                                  const int *__restrict__ sel, int64_t n, int64_t padded, Box<T> *__restrict__ lv0,
                                  int32_t *__restrict__ leaf_id, int32_t *__restrict__ leaf_perm,
                                  Box<T> *__restrict__ lv1) {
   const uint32_t *perm = (sel && *sel) ? perm_b : perm_a;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  // round the loop bound up to whole warps so shuffles see full warps
-  const int64_t limit = ((padded + 31) / 32) * 32;
-  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < limit; j += stride) {
-    Box<T> x = empty_box<T>();
-    if (j < n) {
-      uint32_t r = perm[j];
-      if ((int64_t)r >= n) r = 0;  // only after a timed-out sort (reported by the caller)
-      x = load_box(b, r);
-      leaf_id[j] = ids ? ids[r] : (int32_t)r;
-      leaf_perm[j] = (int32_t)r;
-    } else if (j < padded) {
-      leaf_id[j] = -1;
-      leaf_perm[j] = -1;
-    }
-    if (j < padded) store_box(lv0, j, x);
-    if constexpr (F > 0) {
-      Box<T> u = x;
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  constexpr int64_t kChunk = 32 * kLeafUnroll;
+  for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c * kChunk < padded; c += nwarps) {
+    uint32_t r[kLeafUnroll];
 #pragma unroll
-      for (int o = F / 2; o > 0; o >>= 1) {
-        u.x1 = tmin(u.x1, __shfl_xor_sync(0xffffffffu, u.x1, o));
-        u.y1 = tmin(u.y1, __shfl_xor_sync(0xffffffffu, u.y1, o));
-        u.x2 = tmax(u.x2, __shfl_xor_sync(0xffffffffu, u.x2, o));
-        u.y2 = tmax(u.y2, __shfl_xor_sync(0xffffffffu, u.y2, o));
+    for (int k = 0; k < kLeafUnroll; k++) {
+      const int64_t j = c * kChunk + 32 * k + lane;
+      r[k] = j < n ? perm[j] : 0u;
+      if ((int64_t)r[k] >= n) r[k] = 0;  // only after a timed-out sort (reported by the caller)
+    }
+    Box<T> x[kLeafUnroll];
+#pragma unroll
+    for (int k = 0; k < kLeafUnroll; k++) {
+      const int64_t j = c * kChunk + 32 * k + lane;
+      x[k] = j < n ? load_box(b, r[k]) : empty_box<T>();
+    }
+#pragma unroll
+    for (int k = 0; k < kLeafUnroll; k++) {
+      const int64_t j = c * kChunk + 32 * k + lane;
+      if (j < n) {
+        leaf_id[j] = ids ? ids[r[k]] : (int32_t)r[k];
+        leaf_perm[j] = (int32_t)r[k];
+      } else if (j < padded) {
+        leaf_id[j] = -1;
+        leaf_perm[j] = -1;
       }
-      if ((j % F) == 0 && j < n) store_box(lv1, j / F, u);
+      if (j < padded) store_box(lv0, j, x[k]);
+      if constexpr (F > 0) {
+        Box<T> u = x[k];
+#pragma unroll
+        for (int o = F / 2; o > 0; o >>= 1) {
+          u.x1 = tmin(u.x1, __shfl_xor_sync(0xffffffffu, u.x1, o));
+          u.y1 = tmin(u.y1, __shfl_xor_sync(0xffffffffu, u.y1, o));
+          u.x2 = tmax(u.x2, __shfl_xor_sync(0xffffffffu, u.x2, o));
+          u.y2 = tmax(u.y2, __shfl_xor_sync(0xffffffffu, u.y2, o));
+        }
+        if ((j % F) == 0 && j < n) store_box(lv1, j / F, u);
+      }
     }
   }
 }
@@ -423,7 +593,7 @@ int pack_tree(prt_tree *t, const void *d_boxes, const int32_t *d_ids, const uint
   Box<T> *mbr = reinterpret_cast<Box<T> *>(t->d_mbr);
   Box<T> *lv1 = L.levels > 1 ? mbr + L.offset[1] : nullptr;
   const int block = 256;
-  int g = grid_for(L.padded[0], block, 16);
+  int g = grid_for((L.padded[0] + kLeafUnroll - 1) / kLeafUnroll, block, 8);
   bool fused = false;
   switch (L.levels > 1 ? t->fanout : 0) {
 #define PRT_LEAF_CASE(F)                                                                                 \
@@ -677,7 +847,14 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
     while ((1ll << seg_bits) < nseg) seg_bits++;
     const int use_y = p & 1;
     const uint32_t *cur = have_perm ? perm : nullptr;
-    if (!wide) {
+    if (seg <= kTdLocal) {
+      // short runs: sorted run by run in shared memory, into tmp
+      rc = dispatch_coord(coord_type, [&](auto tag) {
+        using T = decltype(tag);
+        return td_local_level<T>(d_boxes, cur, n, seg, use_y, tmp, s);
+      });
+      std::swap(perm, tmp);
+    } else if (!wide) {
       rc = dispatch_coord(coord_type, [&](auto tag) {
         using T = decltype(tag);
         if constexpr (sizeof(T) == 4) {

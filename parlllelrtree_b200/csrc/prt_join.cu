@@ -40,6 +40,12 @@ struct JoinLevel {
   int td_slots;
 };
 
+// One block iteration takes kJoinRounds rounds of kGroups items per warp: the
+// frontier items of all rounds are loaded first, then their node entries, so
+// each warp has that many independent loads in flight; the hits of the whole
+// iteration are reserved with one atomicAdd per block.
+constexpr int kJoinRounds = 4;
+
 template <typename T, int G>
 __global__ void __launch_bounds__(kJoinBlock) expand_kernel(JoinLevel J, const Box<T> *__restrict__ queries,
                                                             int fanout) {
@@ -48,48 +54,62 @@ __global__ void __launch_bounds__(kJoinBlock) expand_kernel(JoinLevel J, const B
   const int sub = lane / G;           // group within the warp
   const int e = lane % G;             // entry within the node
   constexpr int kGroups = 32 / G;
-  const uint32_t gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (sub * G));
-  int64_t count = J.in ? (int64_t)min((unsigned long long)J.in_cap, *J.in_count) : J.nq;
-  // One output reservation per CTA iteration: the warps' hit counts are
-  // scanned in shared memory (double-buffered by iteration parity) and thread
-  // 0 does the single atomicAdd on the level counter.
   constexpr int kWarps = kJoinBlock / 32;
+  const uint32_t gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (sub * G));
+  const uint32_t lt = lanemask_lt();
+  int64_t count = J.in ? (int64_t)min((unsigned long long)J.in_cap, *J.in_count) : J.nq;
   __shared__ uint32_t s_wcount[2][kWarps];
   __shared__ unsigned long long s_base[2];
   const int warp = threadIdx.x >> 5;
-  const int64_t per_block = (int64_t)kWarps * kGroups;
+  const int64_t per_warp = (int64_t)kJoinRounds * kGroups;
+  const int64_t per_block = (int64_t)kWarps * per_warp;
   int par = 0;
   for (int64_t bb = blockIdx.x * per_block; bb < count; bb += (int64_t)gridDim.x * per_block, par ^= 1) {
-    const int64_t item = bb + warp * kGroups + sub;
-    bool live = item < count;
-    uint32_t q = 0, node = 0;
-    if (live) {
-      if (J.in) {
-        uint2 it = J.in[item];
-        q = it.x;
-        node = it.y;
-      } else {
-        q = (uint32_t)item;
+    const int64_t wb = bb + warp * per_warp;
+    uint32_t q[kJoinRounds], node[kJoinRounds];
+#pragma unroll
+    for (int r = 0; r < kJoinRounds; r++) {
+      const int64_t item = wb + r * kGroups + sub;
+      q[r] = 0;
+      node[r] = 0;
+      if (item < count) {
+        if (J.in) {
+          const uint2 it = J.in[item];
+          q[r] = it.x;
+          node[r] = it.y;
+        } else {
+          q[r] = (uint32_t)item;
+        }
       }
     }
-    const int64_t entry = (int64_t)node * fanout + e;
-    bool hit = false;
-    if (live && e < fanout) {
-      Box<T> qb = load_box(queries, q);
-      Box<T> eb = load_box(mbr, entry);  // padded slots hold a box that intersects nothing
-      hit = overlaps(eb, qb);
+    uint32_t ballots[kJoinRounds];
+    uint32_t wtot = 0;
+#pragma unroll
+    for (int r = 0; r < kJoinRounds; r++) {
+      const int64_t item = wb + r * kGroups + sub;
+      const bool live = item < count;
+      bool hit = false;
+      if (live && e < fanout) {
+        const Box<T> qb = load_box(queries, q[r]);
+        const Box<T> eb = load_box(mbr, (int64_t)node[r] * fanout + e);  // padded slots intersect nothing
+        hit = overlaps(eb, qb);
+      }
+      ballots[r] = __ballot_sync(0xffffffffu, hit);
+      wtot += __popc(ballots[r]);
+      if (J.counts && live && e == 0) {
+        const int k = __popc(ballots[r] & gmask);
+        const int64_t fill = J.td_slots ? fanout : min((int64_t)fanout, J.n_entries - (int64_t)node[r] * fanout);
+        atomicAdd(reinterpret_cast<unsigned long long *>(&J.counts[3 * (int64_t)q[r]]), (unsigned long long)fill);
+        if (k > 1)
+          atomicAdd(reinterpret_cast<unsigned long long *>(&J.counts[3 * (int64_t)q[r] + 1]),
+                    (unsigned long long)(k - 1));
+        if (J.leaf && k)
+          atomicAdd(reinterpret_cast<unsigned long long *>(&J.counts[3 * (int64_t)q[r] + 2]), (unsigned long long)k);
+      }
     }
-    const uint32_t ballot = __ballot_sync(0xffffffffu, hit);
-    if (J.counts && live && e == 0) {
-      int k = __popc(ballot & gmask);
-      int64_t fill = J.td_slots ? fanout : min((int64_t)fanout, J.n_entries - (int64_t)node * fanout);
-      atomicAdd(reinterpret_cast<unsigned long long *>(&J.counts[3 * (int64_t)q]), (unsigned long long)fill);
-      if (k > 1) atomicAdd(reinterpret_cast<unsigned long long *>(&J.counts[3 * (int64_t)q + 1]),
-                           (unsigned long long)(k - 1));
-      if (J.leaf && k) atomicAdd(reinterpret_cast<unsigned long long *>(&J.counts[3 * (int64_t)q + 2]),
-                                 (unsigned long long)k);
-    }
-    if (lane == 0) s_wcount[par][warp] = __popc(ballot);
+    // one reservation per block iteration (warp counts double-buffered by
+    // iteration parity, so one barrier separates the writes and the reads)
+    if (lane == 0) s_wcount[par][warp] = wtot;
     __syncthreads();
     if (threadIdx.x == 0) {
       uint32_t tot = 0;
@@ -98,13 +118,18 @@ __global__ void __launch_bounds__(kJoinBlock) expand_kernel(JoinLevel J, const B
       s_base[par] = tot ? atomicAdd(J.out_count, (unsigned long long)tot) : 0ull;
     }
     __syncthreads();
-    if (hit) {
-      uint32_t woff = 0;
+    if (wtot) {
+      unsigned long long slot = s_base[par];
 #pragma unroll
-      for (int w = 0; w < kWarps; w++) woff += w < warp ? s_wcount[par][w] : 0u;
-      unsigned long long slot = s_base[par] + woff + __popc(ballot & lanemask_lt());
-      if ((int64_t)slot < J.out_cap) {
-        J.out[slot] = J.leaf ? make_uint2((uint32_t)entry, q) : make_uint2(q, (uint32_t)entry);
+      for (int w = 0; w < kWarps; w++) slot += w < warp ? s_wcount[par][w] : 0u;
+#pragma unroll
+      for (int r = 0; r < kJoinRounds; r++) {
+        if (ballots[r] >> lane & 1u) {
+          const unsigned long long at = slot + __popc(ballots[r] & lt);
+          const uint32_t entry = node[r] * (uint32_t)fanout + (uint32_t)e;
+          if ((int64_t)at < J.out_cap) J.out[at] = J.leaf ? make_uint2(entry, q[r]) : make_uint2(q[r], entry);
+        }
+        slot += __popc(ballots[r]);
       }
     }
   }
