@@ -230,9 +230,17 @@ __device__ __forceinline__ uint32_t part1by1_16(uint32_t v) {
 
 // MORTON32: centre of each box on a 65536^2 grid over the data extent; the
 // expression order matches the oracle exactly (no FMA: built with -fmad=false).
+// The four 8-bit digit histograms of the keys are counted on the way (block
+// histograms in shared memory, one global add per nonzero bin), so the sort
+// need not read the keys again to plan its passes.
 template <typename T>
-__global__ void morton32_kernel(const Box<T> *__restrict__ b, int64_t n, const unsigned long long *__restrict__ ext,
-                                uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+__global__ void __launch_bounds__(256) morton32_kernel(const Box<T> *__restrict__ b, int64_t n,
+                                                       const unsigned long long *__restrict__ ext,
+                                                       uint32_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                                                       uint32_t *__restrict__ ghist) {
+  __shared__ uint32_t h[4 * 256];
+  for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) h[i] = 0;
+  __syncthreads();
   const double minX = unord_f64(ext[0]), minY = unord_f64(ext[1]);
   const double maxX = unord_f64(ext[2]), maxY = unord_f64(ext[3]);
   const double ex = (maxX - minX) > (maxY - minY) ? (maxX - minX) : (maxY - minY);
@@ -245,9 +253,15 @@ __global__ void morton32_kernel(const Box<T> *__restrict__ b, int64_t n, const u
     double ty = (cy - minY) * inv;
     uint32_t gx = tx >= 65535.0 ? 65535u : (tx > 0.0 ? (uint32_t)tx : 0u);
     uint32_t gy = ty >= 65535.0 ? 65535u : (ty > 0.0 ? (uint32_t)ty : 0u);
-    keys[i] = part1by1_16(gx) | (part1by1_16(gy) << 1);
+    const uint32_t k = part1by1_16(gx) | (part1by1_16(gy) << 1);
+    keys[i] = k;
     vals[i] = (uint32_t)i;
+#pragma unroll
+    for (int p = 0; p < 4; p++) atomicAdd(&h[p * 256 + ((k >> (8 * p)) & 0xFF)], 1u);
   }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x)
+    if (h[i]) atomicAdd(&ghist[i], h[i]);
 }
 
 // Spreads the low 16 bits of v into 2-bit chunks, one per byte (chunk k ->
@@ -689,15 +703,16 @@ int finish(unsigned *d_err, cudaStream_t s, int rc) {
 // look-back wait gives up.
 int bu_enqueue(prt_tree *t, const void *d_boxes, const int32_t *d_ids, unsigned *err, cudaStream_t s) {
   const int64_t n = t->n;
-  // scratch: ext (4 x 8), err, sel, keys0/1, vals0/1
+  // scratch: ext (4 x 8), err, sel, digit histograms (4 x 256), keys0/1, vals0/1
   unsigned char *scr = nullptr;
   size_t kb = t->key_mode == PRT_KEY_REF64 ? 8 : 4;
-  size_t need = 64 + 2 * kb * n + 2 * 4 * n + 64;
+  size_t need = 64 + 4096 + 2 * kb * n + 2 * 4 * n + 64;
   int rc = dmalloc(reinterpret_cast<void **>(&scr), need, s);
   if (rc) return rc;
   unsigned long long *ext = reinterpret_cast<unsigned long long *>(scr);
   int *sel = reinterpret_cast<int *>(scr + 36);
-  unsigned char *kp = scr + 64;
+  uint32_t *hist = reinterpret_cast<uint32_t *>(scr + 64);
+  unsigned char *kp = scr + 64 + 4096;
   void *keys0 = kp, *keys1 = kp + kb * n;
   uint32_t *vals0 = reinterpret_cast<uint32_t *>(kp + 2 * kb * n);
   uint32_t *vals1 = vals0 + n;
@@ -705,6 +720,11 @@ int bu_enqueue(prt_tree *t, const void *d_boxes, const int32_t *d_ids, unsigned 
   int g = grid_for(n, 256, 16);
   if (e == cudaSuccess) {
     if (t->key_mode == PRT_KEY_MORTON32) {
+      e = cudaMemsetAsync(hist, 0, 4096, s);
+      if (e != cudaSuccess) {
+        dfree(scr, s);
+        return cuda_status(e, "memset");
+      }
       {
         PRT_PROF("extent_init", s);
         extent_init_kernel<<<1, 1, 0, s>>>(ext);
@@ -719,13 +739,13 @@ int bu_enqueue(prt_tree *t, const void *d_boxes, const int32_t *d_ids, unsigned 
         }
         {
           PRT_PROF("morton32", s);
-          morton32_kernel<T><<<g, 256, 0, s>>>(b, n, ext, reinterpret_cast<uint32_t *>(keys0), vals0);
+          morton32_kernel<T><<<g, 256, 0, s>>>(b, n, ext, reinterpret_cast<uint32_t *>(keys0), vals0, hist);
         }
         return PRT_OK;
       });
       if (!rc)
         rc = radix_sort_pairs<uint32_t>(reinterpret_cast<uint32_t *>(keys0), vals0,
-                                        reinterpret_cast<uint32_t *>(keys1), vals1, n, 32, sel, err, s);
+                                        reinterpret_cast<uint32_t *>(keys1), vals1, n, 32, sel, err, s, hist);
     } else {
       long long *ei = reinterpret_cast<long long *>(ext);
       const Box<int64_t> *b = reinterpret_cast<const Box<int64_t> *>(d_boxes);

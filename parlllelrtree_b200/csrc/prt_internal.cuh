@@ -190,10 +190,14 @@ inline int grid_for(int64_t work, int block, int per_sm = 8) {
 // Stable LSD sort of (key, value) pairs; keys are KeyT (uint32_t or
 // uint64_t), values uint32_t.  Bits [0, key_bits) are sorted.  The sorted data
 // ends in either the input or the alternate buffers; *d_sel (device) receives
-// 0 when it is in (keys0, vals0) and 1 for (keys1, vals1).
+// 0 when it is in (keys0, vals0) and 1 for (keys1, vals1).  d_hist, when
+// given, holds the 8-bit digit histograms of every pass (passes x 256, as a
+// key generator can count them while it writes the keys); otherwise the sort
+// reads the keys once to count them.
 template <typename KeyT>
 int radix_sort_pairs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1, int64_t n,
-                     int key_bits, int *d_sel, unsigned *d_err, cudaStream_t s);
+                     int key_bits, int *d_sel, unsigned *d_err, cudaStream_t s,
+                     const uint32_t *d_hist = nullptr);
 
 // Exclusive prefix sum of n values into d_out (int64); *d_total (device,
 // optional) receives the sum.

@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(kSortBlock, PRT_SORT_MIN_BLOCKS) onesweep_pass
 
 template <typename KeyT>
 int radix_sort_pairs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1, int64_t n, int key_bits,
-                     int *d_sel, unsigned *d_err, cudaStream_t s) {
+                     int *d_sel, unsigned *d_err, cudaStream_t s, const uint32_t *d_hist) {
   PRT_CHECK(n >= 0 && n < (int64_t)kCountMask, PRT_ERR_INVALID, "radix sort: n=%lld out of range",
             (long long)n);
   int passes = (key_bits + 7) / 8;
@@ -339,13 +339,13 @@ int radix_sort_pairs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1,
   cudaError_t e = cudaMemsetAsync(scratch, 0, total, s);
   if (e == cudaSuccess) {
     int g = grid_for(n, 256, 4);
-    {
+    if (!d_hist) {
       PRT_PROF("hist", s);
       hist_kernel<KeyT><<<g, 256, sizeof(uint32_t) * passes * kRadix, s>>>(keys0, n, passes, ghist);
     }
     {
       PRT_PROF("plan", s);
-      plan_kernel<<<1, kRadix, 0, s>>>(ghist, goff, passes, n, plan, d_sel);
+      plan_kernel<<<1, kRadix, 0, s>>>(d_hist ? d_hist : ghist, goff, passes, n, plan, d_sel);
     }
     size_t smem = sizeof(PassSmem<KeyT>);
     // the shared-memory opt-in is set once per device (not a stream
@@ -381,9 +381,9 @@ std::atomic<int> g_wait_blind{0};
 WaitLimit wait_limit() { return WaitLimit{g_wait_polls.load(), g_wait_blind.load()}; }
 
 template int radix_sort_pairs<uint32_t>(uint32_t *, uint32_t *, uint32_t *, uint32_t *, int64_t, int, int *,
-                                        unsigned *, cudaStream_t);
+                                        unsigned *, cudaStream_t, const uint32_t *);
 template int radix_sort_pairs<uint64_t>(uint64_t *, uint32_t *, uint64_t *, uint32_t *, int64_t, int, int *,
-                                        unsigned *, cudaStream_t);
+                                        unsigned *, cudaStream_t, const uint32_t *);
 
 }  // namespace prt
 
