@@ -11,11 +11,16 @@ whole 10M-box array; `value` = boxes of all ranks / max-over-ranks device time
 per step, in Mboxes/s.  Inputs (160 MB) are larger than the 126 MB L2 and L2
 is also flushed (256 MB write) between timed steps.
 
-Reported beside it (same JSON line): the other builds of that configuration
-(bottom-up/top-down at fanout 16 and 32), 1M window queries (side uniform
-1e-4..1e-2) joined against the fanout-16 tree, and the small overlay
-configuration (2 x 10,000 stars, 8-32 vertices, radius log-uniform 1e-3..1e-2)
-clipped with the plain and the batched schedule.
+Reported beside it (same JSON line, `secondary`): the other builds of that
+configuration (bottom-up/top-down at fanout 16 and 32); 1M window queries
+(side uniform 1e-4..1e-2) joined against the fanout-16 tree, with the join's
+HBM roofline; the batched uneven overlay at its full size (2 x 1M stars, ~4M
+candidate pairs: batched schedule, graph pipeline, plain schedule on a
+labelled strided subset, 400 pairs checked bit for bit against the oracle);
+the differentiable-area configuration (1M pairs, forward and adjoint, the
+adjoint's HBM roofline); the map-alignment loop (200k parcels x 200 steps);
+and the small overlay configuration (2 x 10,000 stars, 8-32 vertices, radius
+log-uniform 1e-3..1e-2) clipped with the plain and the batched schedule.
 
 --impl reference times the reference's own CPU build (BotomUp-rtree.cu:776-833,
 qsort + packing, built from its sources into oracle/_ref) on the same boxes
@@ -530,16 +535,29 @@ def alignment(n: int = 200_000):
     and quadrilaterals), the second layer under a random affine (rotation
     +-2 deg, scale +-1%, translation +-0.005) plus vertex noise sigma 1e-4;
     200 Adam steps, each rebuilding the R-tree, joining, clipping and running
-    the area adjoint (parlllelrtree_b200.alignment).  Reports steps/s from the
-    device time of the steps (CUDA events per pyramid stage) and the
-    recovery error."""
+    the area adjoint (parlllelrtree_b200.alignment).  `loop_s` is the time
+    between CUDA events at the start and end of each pyramid stage, summed:
+    it includes the host's work between launches (Python, torch's small ops,
+    the library's count read-backs), which bounds this loop.  A second run
+    with the library's launch profiler on gives `kernel_s`, the device time of
+    the library's own kernels alone.  Also the recovery error."""
+    from parlllelrtree_b200 import _lib
     from parlllelrtree_b200 import alignment as al
 
     A, B, T = al.parcel_layers(n, seed=3)
     theta, rec, stage_s = al.fit_affine(A, B, steps=200)
     total = sum(stage_s)
-    return {"parcels": n, "steps": len(rec), "device_s": total, "steps_s": len(rec) / total,
+    _lib.profile_reset()
+    _lib.profile_enable(1)
+    al.fit_affine(A, B, steps=200)
+    _lib.profile_enable(0)
+    prof = _lib.profile_read()
+    _lib.profile_reset()
+    kernel_ms = sum(v[0] for v in prof.values())
+    top = sorted(prof.items(), key=lambda kv: -kv[1][0])[:6]
+    return {"parcels": n, "steps": len(rec), "loop_s": total, "steps_s": len(rec) / total,
             "stage_s": stage_s, "full_res_ms_per_step": stage_s[-1] / 50 * 1e3,
+            "kernel_s": kernel_ms * 1e-3, "kernel_ms_top": {k: round(v[0], 2) for k, v in top},
             "recovery_error": al.recovery_error(theta, T), "initial_error": al.recovery_error(np.zeros(6), T),
             "final_overlap": rec[-1]["overlap"]}
 
@@ -603,8 +621,9 @@ def batched_overlay(prt, scale: float = 1.0, plain_stride: int = 32):
     HBM; after an untimed warm-up on a 1% strided subset that sizes the
     allocator pools), and the whole build-join-clip graph (prt.Pipeline) on a
     side stream.  The plain schedule (one thread per pair in join order) is
-    timed on an evenly strided subset (every plain_stride-th pair, labelled):
-    on the full list it takes ~8 minutes.  Parity: 400 evenly strided pairs of
+    timed on an evenly strided subset (every plain_stride-th pair, labelled;
+    on the full list it takes ~8 minutes), and the batched schedule on the
+    same subset: batched_over_plain compares the two on equal work.  Parity: 400 evenly strided pairs of
     the batched results against the oracle's GPC clip, contour for contour and
     bit for bit; the same pairs give the CPU baseline."""
     import torch
@@ -658,7 +677,13 @@ def batched_overlay(prt, scale: float = 1.0, plain_stride: int = 32):
     out["plain_pairs_s"] = len(sub) / (ms_p * 1e-3)
     out["plain_nonempty"] = r.nonempty
     del r
-    out["batched_over_plain"] = out["batched_pairs_s"] / out["plain_pairs_s"]
+    # the batched schedule on the same subset: the ratio compares equal work
+    ms_b, r = timed(lambda: prt.overlay(sub, LA, LB, leaf_to_poly=l2p, sched="batched"))
+    out["subset_batched_ms"] = ms_b
+    out["subset_batched_pairs_s"] = len(sub) / (ms_b * 1e-3)
+    out["subset_matches_plain"] = bool(r.nonempty == out["plain_nonempty"])
+    del r
+    out["batched_over_plain"] = out["subset_batched_pairs_s"] / out["plain_pairs_s"]
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
         pipe = prt.Pipeline(LA, LB, max_pairs=int(np_ * 1.25) + 1024)

@@ -295,7 +295,9 @@ int prt_clip_pair_host(int op, int s_ncont, const int32_t *s_nverts, const doubl
  * warps_per_sm persistent warps per SM (at most 12, the resident limit);
  * every warp takes the next pair (warp mode) or the next 32 pairs (thread
  * mode) of the largest bin that still has pairs, so the largest pairs are
- * clipped first by all warps. */
+ * clipped first by all warps.  A launch whose thread-mode pairs would fill
+ * less than half a wave of warps one pair per thread clips every pair in warp
+ * mode instead (same output, more warps in flight). */
 #define PRT_MAX_BINS 8
 typedef struct {
   int32_t nbins;

@@ -720,9 +720,15 @@ __global__ void __launch_bounds__(32 * kBwdWarps, 4) area_bwd_kernel(
 // (polygons above kBwdMaxV vertices or 31 rings, unclean crossings, slivers
 // whose area the bound does not pin to kFwdTol, ids out of range) is listed in
 // fb[] for the GPC clip.  GPC intersects the same edges, so for a clean pair
-// the two areas differ only by the rounding of the crossing vertices, which
-// the bound covers with a factor of 8.
-constexpr double kFwdTol = 1e-11;
+// the two areas differ only by where each side rounds the crossing vertices:
+// a vertex moves by at most ~2 eps max|coordinate| / sin(angle), which moves
+// the area by that times the crossing edges' lengths.  pair_boundary sums
+// (|r|_1 + |s|_1) / sin over the crossings as seen from both edges (each
+// crossing twice, and 1-norms, which are at least the lengths), so
+// 2 eps max|coordinate| times the sum bounds the difference; a pair is kept
+// when that is below kFwdTol of its area, ten times inside the 1e-9 the
+// forward promises.
+constexpr double kFwdTol = 1e-10;
 
 // Pairs the last forward call listed for the GPC clip (prt_area_fwd_fallbacks).
 std::atomic<int64_t> g_fwd_fallbacks{0};
@@ -779,7 +785,7 @@ __global__ void __launch_bounds__(32 * kBwdWarps, 4) area_fwd_kernel(
       }
       const float cmax = fmaxf(fmaxf(fmaxf(fabsf(ext[0].x), fabsf(ext[0].y)), fmaxf(fabsf(ext[0].z), fabsf(ext[0].w))),
                                fmaxf(fmaxf(fabsf(ext[1].x), fabsf(ext[1].y)), fmaxf(fabsf(ext[1].z), fabsf(ext[1].w))));
-      const double bound = 8.0 * 2.220446049250313e-16 * (double)cmax * er;
+      const double bound = 2.0 * 2.220446049250313e-16 * (double)cmax * er;
       const double ar = 0.5 * a2;
       if (bound <= kFwdTol * fabs(ar)) {
         if (lane == 0) area[i] = ar;

@@ -383,6 +383,7 @@ template <typename K>
 struct TdLocalSmem {
   K key[2][kTdLocal];
   uint32_t val[2][kTdLocal];
+  uint16_t run[2][kTdLocal];  // run within the tile, moved with its item
   uint32_t wh[8][256];
   uint32_t dstart[256];
   uint32_t wsum[8];
@@ -408,6 +409,7 @@ __global__ void __launch_bounds__(256) td_local_sort_kernel(const Box<T> *__rest
     const T v = __ldg(&c[4 * (int64_t)r + (use_y ? 1 : 0)]);
     S.key[0][i] = (K)ukey(v);
     S.val[0][i] = r;
+    S.run[0][i] = (uint16_t)(i / seg);
   }
   __syncthreads();
   const int total_bits = kKeyBits + run_bits;
@@ -416,10 +418,11 @@ __global__ void __launch_bounds__(256) td_local_sort_kernel(const Box<T> *__rest
   for (int shift = 0; shift < total_bits; shift += 8) {
     for (int i = tid; i < 8 * 256; i += 256) (&S.wh[0][0])[i] = 0;
     __syncthreads();
-    // digit of item i: the key's byte, or above the key the run index
+    // digit of the item at position i: the key's byte, or above the key the
+    // run index (positions change from pass to pass; the run moves along)
     auto digit = [&](int i) -> int {
       if (shift < kKeyBits) return (int)((S.key[cur][i] >> shift) & 0xFF);
-      return (int)(((int64_t)i / seg >> (shift - kKeyBits)) & 0xFF);
+      return (int)((S.run[cur][i] >> (shift - kKeyBits)) & 0xFF);
     };
     int dg[kTdItems];
     uint32_t rk[kTdItems];
@@ -476,6 +479,7 @@ __global__ void __launch_bounds__(256) td_local_sort_kernel(const Box<T> *__rest
         const uint32_t pos = S.dstart[dg[j]] + S.wh[warp][dg[j]] + rk[j];
         S.key[1 - cur][pos] = S.key[cur][i];
         S.val[1 - cur][pos] = S.val[cur][i];
+        S.run[1 - cur][pos] = S.run[cur][i];
       }
     }
     cur = 1 - cur;

@@ -617,8 +617,20 @@ static int run_batched(OverlayState &st, const int64_t *d_idx, int64_t count, in
   BinPlan plan;
   int64_t counts[PRT_MAX_BINS];
   for (int b = 0; b < nb; b++) counts[b] = hb[b + 1] - hb[b];
+  // Too few pairs to keep the GPU busy one per thread (under half a wave of
+  // the thread-only launch, e.g. the 2 x 10,000-star overlay's ~21k pairs in
+  // ~650 warps): clip every pair with a whole warp instead, so there are as
+  // many warps as pairs.  Both clippers give the same output.
+  prt_schedule run_sc = sc;
+  {
+    int64_t thread_warps = 0;
+    for (int b = 0; b < nb; b++)
+      if (!sc.bin_warp_mode[b]) thread_warps += (counts[b] + 31) / 32;
+    if (thread_warps > 0 && thread_warps < (int64_t)kSMs * kLptThreadWarpsPerSM / 2)
+      for (int b = 0; b < nb; b++) run_sc.bin_warp_mode[b] = 1;
+  }
   size_t smem = 0;
-  const size_t bytes = plan_bins(sc, counts, hm, arena_budget(), plan, &smem, scale, true);
+  const size_t bytes = plan_bins(run_sc, counts, hm, arena_budget(), plan, &smem, scale, true);
   plan.n_pairs = st.n;
   for (int b = 0; b < nb; b++) {
     plan.begin[b] = hb[b];

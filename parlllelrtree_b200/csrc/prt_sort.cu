@@ -24,10 +24,10 @@ constexpr int kRadix = 256;
 constexpr int kSortBlock = 256;
 constexpr int kSortWarps = kSortBlock / 32;
 #ifndef PRT_SORT_ITEMS
-#define PRT_SORT_ITEMS 12  // keys per thread of a tile
+#define PRT_SORT_ITEMS 16  // keys per thread of a tile
 #endif
 #ifndef PRT_SORT_MIN_BLOCKS
-#define PRT_SORT_MIN_BLOCKS 4  // resident blocks per SM the pass is compiled for
+#define PRT_SORT_MIN_BLOCKS 3  // resident blocks per SM the pass is compiled for
 #endif
 constexpr int kItems = PRT_SORT_ITEMS;
 constexpr int kTile = kSortBlock * kItems;
@@ -114,15 +114,14 @@ struct PassSmem {
   KeyT keys[kTile];
   uint32_t vals[kTile];
   uint32_t warp_hist[kSortWarps][kRadix];
-  uint32_t tile_count[kRadix];   // digit histogram of the tile (published early)
   uint32_t digit_start[kRadix];  // tile-local exclusive start of each digit
   uint32_t global_start[kRadix];
-  uint32_t scan_tmp[kRadix];
+  uint32_t scan_tmp[kSortWarps];
   int tile;
 };
 
 #ifndef PRT_SORT_LOOKBATCH
-#define PRT_SORT_LOOKBATCH 16
+#define PRT_SORT_LOOKBATCH 8
 #endif
 #ifndef PRT_SORT_BACKOFF_NS
 #define PRT_SORT_BACKOFF_NS 0  // pause between look-back polls that found nothing new
@@ -149,83 +148,73 @@ __global__ void __launch_bounds__(kSortBlock, PRT_SORT_MIN_BLOCKS) onesweep_pass
   const int d = tid;  // kSortBlock == kRadix: thread d owns digit d
   if (tid == 0) S.tile = (int)atomicAdd(tile_ticket, 1u);
   for (int i = tid; i < kSortWarps * kRadix; i += kSortBlock) (&S.warp_hist[0][0])[i] = 0;
-  S.tile_count[d] = 0;
   __syncthreads();
   const int tile = S.tile;
   const int64_t base = (int64_t)tile * kTile;
-  const int64_t wbase = base + (int64_t)warp * 32 * kItems;
+  const int valid = (int)min((int64_t)kTile, n - base);
+  const int wb = warp * 32 * kItems;  // this warp's first item in the tile
 
   KeyT k[kItems];
   uint32_t v[kItems];
-  int dig[kItems];
-  uint32_t rank[kItems];
 #pragma unroll
   for (int i = 0; i < kItems; i++) {
-    int64_t idx = wbase + i * 32 + lane;
-    if (idx < n) {
-      k[i] = src_k[idx];
-      v[i] = src_v[idx];
-      dig[i] = (int)((k[i] >> shift) & 0xFF);
-    } else {
-      k[i] = 0;
-      v[i] = 0;
-      dig[i] = kRadix + lane;  // unique: no peers, never counted
+    const int li = wb + i * 32 + lane;
+    k[i] = 0;
+    v[i] = 0;
+    if (li < valid) {
+      k[i] = src_k[base + li];
+      v[i] = src_v[base + li];
     }
   }
-  // 1. tile histogram by shared atomics, published at once so that later
-  //    tiles' look-back finds it while this tile is still ranking
-#pragma unroll
-  for (int i = 0; i < kItems; i++)
-    if (dig[i] < kRadix) atomicAdd(&S.tile_count[dig[i]], 1u);
-  __syncthreads();
-  const uint32_t total = S.tile_count[d];
-  uint32_t *st = status + (int64_t)tile * kRadix + d;
-  if (tile == 0) atomicExch(st, kFlagPrefix | ((goff[d] + total) & kCountMask));
-  else atomicExch(st, kFlagAgg | (total & kCountMask));
-
-  // 2. stable ranks: warp multisplit
+  // 1. stable ranks and the warps' digit histograms in one sweep: lanes with
+  //    the same digit are found by one ballot per digit bit; the lowest of
+  //    them reads and bumps the warp's counter, the others get the old count
+  //    by shuffle.  Items are ranked in index order (item slot i of lane l is
+  //    tile position wb + 32 i + l), which makes the pass stable.
   const uint32_t lt = lanemask_lt();
   uint32_t *wh = S.warp_hist[warp];
+  uint32_t dr[kItems];  // rank << 9 | digit (256 + lane: no item)
 #pragma unroll
   for (int i = 0; i < kItems; i++) {
-    // lanes holding the same digit: the lowest one reads and bumps the warp's
-    // counter for it, the others get the old count by shuffle
-    // lanes with the same 8-bit digit: AND of one ballot per digit bit
-    const bool ok = dig[i] < kRadix;
+    const int li = wb + i * 32 + lane;
+    const bool ok = li < valid;
+    const uint32_t dg = ok ? (uint32_t)((k[i] >> shift) & 0xFF) : 256u + lane;
     uint32_t peers = __ballot_sync(0xffffffffu, ok);
 #pragma unroll
     for (int b = 0; b < 8; b++) {
-      const uint32_t m = __ballot_sync(0xffffffffu, (dig[i] >> b) & 1);
-      peers &= ((dig[i] >> b) & 1) ? m : ~m;
+      const uint32_t m = __ballot_sync(0xffffffffu, (dg >> b) & 1u);
+      peers &= ((dg >> b) & 1u) ? m : ~m;
     }
     if (!ok) peers = 1u << lane;
     const int leader = __ffs(peers) - 1;
     uint32_t cnt = 0;
-    if (lane == leader && dig[i] < kRadix) {
-      cnt = wh[dig[i]];
-      wh[dig[i]] = cnt + __popc(peers);
+    if (lane == leader && ok) {
+      cnt = wh[dg];
+      wh[dg] = cnt + __popc(peers);
     }
     cnt = __shfl_sync(0xffffffffu, cnt, leader);
-    rank[i] = cnt + __popc(peers & lt);
+    dr[i] = ((cnt + __popc(peers & lt)) << 9) | dg;
     __syncwarp();  // this item's counter updates before the next item's reads
   }
   __syncthreads();
-  // per digit: exclusive prefix over warps
-  {
-    uint32_t run = 0;
+  // 2. digit d: exclusive prefix over the warps and the tile's count, which
+  //    is published at once for the later tiles' look-back
+  uint32_t total = 0;
 #pragma unroll
-    for (int w = 0; w < kSortWarps; w++) {
-      uint32_t c = S.warp_hist[w][d];
-      S.warp_hist[w][d] = run;
-      run += c;
-    }
+  for (int w = 0; w < kSortWarps; w++) {
+    const uint32_t c = S.warp_hist[w][d];
+    S.warp_hist[w][d] = total;
+    total += c;
   }
+  uint32_t *st = status + (int64_t)tile * kRadix + d;
+  if (tile == 0) atomicExch(st, kFlagPrefix | ((goff[d] + total) & kCountMask));
+  else atomicExch(st, kFlagAgg | (total & kCountMask));
   // tile-local exclusive scan over digits: shuffle scan per warp of 32
   // digits, then the 8 warp totals
   uint32_t incl = total;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += t;
   }
   if (lane == 31) S.scan_tmp[warp] = incl;
@@ -235,18 +224,19 @@ __global__ void __launch_bounds__(kSortBlock, PRT_SORT_MIN_BLOCKS) onesweep_pass
   for (int w = 0; w < kSortWarps; w++) woff += w < warp ? S.scan_tmp[w] : 0u;
   S.digit_start[d] = woff + incl - total;
   __syncthreads();
-  // stage the tile in digit order before the look-back: the items leave the
-  // registers, which the look-back's wide batches then use
+  // 3. stage the tile in digit order before the look-back: the items leave
+  //    the registers, which the look-back's batches then use
 #pragma unroll
   for (int i = 0; i < kItems; i++) {
-    if (dig[i] < kRadix) {
-      uint32_t pos = S.digit_start[dig[i]] + S.warp_hist[warp][dig[i]] + rank[i];
+    const uint32_t dg = dr[i] & 511u;
+    if (dg < 256u) {
+      const uint32_t pos = S.digit_start[dg] + wh[dg] + (dr[i] >> 9);
       S.keys[pos] = k[i];
       S.vals[pos] = v[i];
     }
   }
 
-  // 3. decoupled look-back for digit d, kLookBatch predecessor statuses per
+  // 4. decoupled look-back for digit d, kLookBatch predecessor statuses per
   //    round trip; every wait is bounded
   uint32_t excl = goff[d];
   if (tile > 0) {
@@ -255,21 +245,21 @@ __global__ void __launch_bounds__(kSortBlock, PRT_SORT_MIN_BLOCKS) onesweep_pass
     int spins = 0;
     bool timed_out = false;
     for (;;) {
-      uint32_t s[kLookBatch];
+      uint32_t sv[kLookBatch];
 #pragma unroll
       for (int j = 0; j < kLookBatch; j++) {
         uint32_t sj = 2u << 30;  // before tile 0: an empty prefix (never reached)
         if (t - j >= 0) sj = *reinterpret_cast<volatile uint32_t *>(status + (int64_t)(t - j) * kRadix + d);
-        s[j] = wl.blind ? 0u : sj;
+        sv[j] = wl.blind ? 0u : sj;
       }
       int used = 0;
       bool done = false;
 #pragma unroll
       for (int j = 0; j < kLookBatch; j++) {
         if (done || used < j) continue;  // stop at the first prefix or unpublished status
-        const uint32_t f = s[j] & ~kCountMask;
+        const uint32_t f = sv[j] & ~kCountMask;
         if (f == 0u) continue;           // not yet published: retry from here
-        acc += s[j] & kCountMask;
+        acc += sv[j] & kCountMask;
         used = j + 1;
         if (f == kFlagPrefix) done = true;
       }
@@ -291,14 +281,12 @@ __global__ void __launch_bounds__(kSortBlock, PRT_SORT_MIN_BLOCKS) onesweep_pass
   S.global_start[d] = excl - S.digit_start[d];
   __syncthreads();
 
-  // 4. write the staged tile out in coalesced runs per digit
-  int64_t valid = n - base;
-  if (valid > kTile) valid = kTile;
-  // (a look-back that timed out leaves the offsets wrong: the bound keeps
-  // every write inside the buffers, and the caller reports the timeout)
+  // 5. write the staged tile out in coalesced runs per digit (a look-back
+  //    that timed out leaves the offsets wrong: the bound keeps every write
+  //    inside the buffers, and the caller reports the timeout)
   for (int i = tid; i < valid; i += kSortBlock) {
-    KeyT kk = S.keys[i];
-    int dd = (int)((kk >> shift) & 0xFF);
+    const KeyT kk = S.keys[i];
+    const int dd = (int)((kk >> shift) & 0xFF);
     const uint32_t dst = S.global_start[dd] + (uint32_t)i;
     if ((int64_t)dst < n) {
       dst_k[dst] = kk;

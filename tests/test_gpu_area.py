@@ -204,7 +204,7 @@ def test_forward_differentiable_configuration(cuda):
     area = prt.intersection_area(LA, LB, idx, idx).cpu().numpy()
     fb = ctypes.c_int64(-1)
     _lib.check(_lib.lib().prt_area_fwd_fallbacks(ctypes.byref(fb)))
-    assert fb.value < 0.05 * n
+    assert fb.value < 0.1 * n  # most pairs on the boundary-integral path
     A = {k: v.cpu().numpy() for k, v in Ad.items()}
     B = {k: v.cpu().numpy() for k, v in Bd.items()}
     for i in range(n):
