@@ -324,8 +324,8 @@ def run_ours(args):
         # one radix pass moves every (key, value): read 4 + 4 B, write 4 + 4 B
         "onesweep_pass": 16 * N_BOXES,
         # gather of a 16 B box by index + 4 B index read + 16 B entry + 4 B id
-        # + 4 B leaf perm writes
-        "pack_leaf": 44 * N_BOXES,
+        # writes
+        "pack_leaf": 40 * N_BOXES,
         "morton32": 24 * N_BOXES,
         "hist": 4 * N_BOXES,
     }.get(dom_name)

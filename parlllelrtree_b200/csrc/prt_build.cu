@@ -528,8 +528,7 @@ template <typename T, int F>
 __global__ void __launch_bounds__(256) pack_leaf_kernel(const Box<T> *__restrict__ b, const int32_t *__restrict__ ids,
                                  const uint32_t *__restrict__ perm_a, const uint32_t *__restrict__ perm_b,
                                  const int *__restrict__ sel, int64_t n, int64_t padded, Box<T> *__restrict__ lv0,
-                                 int32_t *__restrict__ leaf_id, int32_t *__restrict__ leaf_perm,
-                                 Box<T> *__restrict__ lv1) {
+                                 int32_t *__restrict__ leaf_id, Box<T> *__restrict__ lv1) {
   const uint32_t *perm = (sel && *sel) ? perm_b : perm_a;
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -551,13 +550,8 @@ __global__ void __launch_bounds__(256) pack_leaf_kernel(const Box<T> *__restrict
 #pragma unroll
     for (int k = 0; k < kLeafUnroll; k++) {
       const int64_t j = c * kChunk + 32 * k + lane;
-      if (j < n) {
-        leaf_id[j] = ids ? ids[r[k]] : (int32_t)r[k];
-        leaf_perm[j] = (int32_t)r[k];
-      } else if (j < padded) {
-        leaf_id[j] = -1;
-        leaf_perm[j] = -1;
-      }
+      if (j < n) leaf_id[j] = ids ? ids[r[k]] : (int32_t)r[k];
+      else if (j < padded) leaf_id[j] = -1;
       if (j < padded) store_box(lv0, j, x[k]);
       if constexpr (F > 0) {
         Box<T> u = x[k];
@@ -618,7 +612,7 @@ int pack_tree(prt_tree *t, const void *d_boxes, const int32_t *d_ids, const uint
   case F: {                                                                                              \
     PRT_PROF("pack_leaf", s);                                                                            \
     pack_leaf_kernel<T, F><<<g, block, 0, s>>>(b, d_ids, perm_a, perm_b, d_sel, t->n, L.padded[0], mbr, \
-                                               t->d_leaf_id, t->d_perm, lv1 ? lv1 : mbr);                \
+                                               t->d_leaf_id, lv1 ? lv1 : mbr);                           \
     fused = lv1 != nullptr;                                                                              \
     break;                                                                                               \
   }
@@ -632,7 +626,7 @@ int pack_tree(prt_tree *t, const void *d_boxes, const int32_t *d_ids, const uint
       {
         PRT_PROF("pack_leaf", s);
         pack_leaf_kernel<T, 0><<<g, block, 0, s>>>(b, d_ids, perm_a, perm_b, d_sel, t->n, L.padded[0], mbr,
-                                                 t->d_leaf_id, t->d_perm, nullptr);
+                                                 t->d_leaf_id, nullptr);
       }
   }
   for (int l = 1; l < L.levels; l++) {
@@ -673,11 +667,9 @@ int new_tree(const void *d_boxes, int coord, int64_t n, int fanout, int kind, in
   size_t bs = 4 * coord_size(coord);
   int rc = dmalloc(&t->d_mbr, bs * t->lv.total, s);
   if (!rc) rc = dalloc(&t->d_leaf_id, t->lv.padded[0], s);
-  if (!rc) rc = dalloc(&t->d_perm, t->lv.padded[0], s);
   if (rc) {
     dfree(t->d_mbr, s);
     dfree(t->d_leaf_id, s);
-    dfree(t->d_perm, s);
     delete t;
     return rc;
   }
@@ -958,7 +950,6 @@ int prt_tree_free(prt_tree *t) {
   if (!t) return PRT_OK;
   cudaFreeAsync(t->d_mbr, 0);
   cudaFreeAsync(t->d_leaf_id, 0);
-  cudaFreeAsync(t->d_perm, 0);
   cudaGetLastError();
   delete t;
   return PRT_OK;

@@ -244,6 +244,5 @@ struct prt_tree {
   prt::TreeLevels lv;
   void *d_mbr;          // Box<T>[lv.total], level after level
   int32_t *d_leaf_id;   // record id per leaf entry
-  int32_t *d_perm;      // record index per leaf entry
   int device;
 };
