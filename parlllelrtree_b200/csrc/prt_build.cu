@@ -323,6 +323,20 @@ __global__ void td_key32_kernel(const Box<T> *__restrict__ b, const uint32_t *__
   }
 }
 
+// Top-down level with a single run (the first level when one run holds all
+// records), 32-bit coordinates: the key is the coordinate alone.
+template <typename T>
+__global__ void td_key32u_kernel(const Box<T> *__restrict__ b, const uint32_t *__restrict__ perm, int64_t n,
+                                 int use_y, uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t r = perm ? perm[i] : (uint32_t)i;
+    if ((int64_t)r >= n) r = 0;  // only after a timed-out sort (reported by the caller)
+    Box<T> x = load_box(b, r);
+    keys[i] = ukey(use_y ? x.y1 : x.x1);
+    vals[i] = r;
+  }
+}
+
 // Top-down level, 64-bit coordinates, first stage: key = coordinate, value = position.
 template <typename T>
 __global__ void td_key64_kernel(const Box<T> *__restrict__ b, const uint32_t *__restrict__ perm, int64_t n,
@@ -870,6 +884,22 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
         return td_local_level<T>(d_boxes, cur, n, seg, use_y, tmp, s);
       });
       std::swap(perm, tmp);
+    } else if (!wide && seg_bits == 0) {
+      // one run: a stable sort by the 32-bit coordinate alone
+      uint32_t *kk0 = reinterpret_cast<uint32_t *>(k0), *kk1 = reinterpret_cast<uint32_t *>(k1);
+      rc = dispatch_coord(coord_type, [&](auto tag) {
+        using T = decltype(tag);
+        if constexpr (sizeof(T) == 4) {
+          PRT_PROF("td_key32", s);
+          td_key32u_kernel<T><<<g, 256, 0, s>>>(reinterpret_cast<const Box<T> *>(d_boxes), cur, n, use_y, kk0, v0);
+        }
+        return PRT_OK;
+      });
+      if (!rc) rc = radix_sort_pairs<uint32_t>(kk0, v0, kk1, v1, n, 32, sel, err, s);
+      if (!rc) {
+        PRT_PROF("select_copy_u32", s);
+        select_copy_u32_kernel<<<g, 256, 0, s>>>(v0, v1, sel, n, perm);
+      }
     } else if (!wide) {
       rc = dispatch_coord(coord_type, [&](auto tag) {
         using T = decltype(tag);
