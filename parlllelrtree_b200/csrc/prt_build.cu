@@ -667,6 +667,8 @@ int new_tree(const void *d_boxes, int coord, int64_t n, int fanout, int kind, in
   PRT_CHECK(out != nullptr, PRT_ERR_INVALID, "out is NULL");
   *out = nullptr;
   PRT_CHECK(d_boxes != nullptr || n == 0, PRT_ERR_INVALID, "d_boxes is NULL");
+  PRT_CHECK((reinterpret_cast<uintptr_t>(d_boxes) & 15) == 0, PRT_ERR_INVALID,
+            "d_boxes must be 16-byte aligned (boxes are read as 16-byte vectors)");
   PRT_CHECK(n >= 1 && n < (1ll << 30), PRT_ERR_INVALID, "n=%lld outside [1, 2^30)", (long long)n);
   PRT_CHECK(fanout >= 2 && fanout <= 32, PRT_ERR_INVALID, "fanout %d outside [2, 32]", fanout);
   PRT_CHECK(coord >= 0 && coord <= 3, PRT_ERR_INVALID, "coordinate type %d", coord);

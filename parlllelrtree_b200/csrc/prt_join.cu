@@ -206,6 +206,8 @@ int run_join(const prt_tree *t, const void *d_queries, int coord, int64_t nq, ui
             t->coord);
   PRT_CHECK(nq >= 0 && nq < (1ll << 31), PRT_ERR_INVALID, "nq=%lld", (long long)nq);
   PRT_CHECK(cap >= 0, PRT_ERR_INVALID, "cap < 0");
+  PRT_CHECK((reinterpret_cast<uintptr_t>(d_queries) & 15) == 0 && (reinterpret_cast<uintptr_t>(d_pairs) & 7) == 0,
+            PRT_ERR_INVALID, "d_queries must be 16-byte and d_pairs 8-byte aligned");
   if (h_count) *h_count = 0;
   if (nq == 0) return PRT_OK;
   const TreeLevels &L = t->lv;
@@ -463,6 +465,8 @@ int prt_join_noalloc(const prt_tree *t, const void *d_queries, int coord_type, i
             coord_type, t->coord);
   PRT_CHECK(nq >= 0 && nq < (1ll << 31), PRT_ERR_INVALID, "nq=%lld", (long long)nq);
   PRT_CHECK(cap >= 0 && (cap == 0 || d_pairs != nullptr), PRT_ERR_INVALID, "pair buffer");
+  PRT_CHECK((reinterpret_cast<uintptr_t>(d_queries) & 15) == 0 && (reinterpret_cast<uintptr_t>(d_pairs) & 7) == 0,
+            PRT_ERR_INVALID, "d_queries must be 16-byte and d_pairs 8-byte aligned");
   PRT_CHECK(t->lv.levels + 2 <= (int)(kNoAllocCounterBytes / 8), PRT_ERR_INVALID, "tree too deep");
   if (h_count) *h_count = 0;
   if (nq == 0) return PRT_OK;

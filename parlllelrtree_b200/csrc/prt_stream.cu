@@ -60,18 +60,20 @@ __global__ void compact_vertices_kernel(const int64_t *__restrict__ src, const i
 int results_compact(const prt_results *r, cudaStream_t s, void **block, int64_t **pair_off, int32_t **nverts,
                     int32_t **hole, double **xy) {
   const int64_t n = r->n_pairs, nc = r->n_cont, nv = r->n_vert;
-  // layout: pair_off (n+1) | src (nc) | vert_off (nc+1) | xy (2 nv) | nverts (nc) | hole (nc)
-  const size_t b_off = 8 * (size_t)(n + 1), b_src = 8 * (size_t)nc, b_voff = 8 * (size_t)(nc + 1);
-  const size_t b_xy = 16 * (size_t)nv, b_nv = 4 * (size_t)nc;
+  // layout: pair_off (n+1) | src (nc) | vert_off (nc+1) | xy (2 nv) | nverts (nc) | hole (nc),
+  // each part starting on a 256-byte boundary (xy is moved as 16-byte pairs)
+  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t b_off = up(8 * (size_t)(n + 1)), b_src = up(8 * (size_t)nc), b_voff = up(8 * (size_t)(nc + 1));
+  const size_t b_xy = up(16 * (size_t)nv), b_nv = up(4 * (size_t)nc);
   unsigned char *p = nullptr;
-  int rc = dmalloc(reinterpret_cast<void **>(&p), b_off + b_src + b_voff + b_xy + 2 * b_nv + 64, s);
+  int rc = dmalloc(reinterpret_cast<void **>(&p), b_off + b_src + b_voff + b_xy + 2 * b_nv, s);
   if (rc) return rc;
   int64_t *off = reinterpret_cast<int64_t *>(p);
   int64_t *src = reinterpret_cast<int64_t *>(p + b_off);
   int64_t *voff = reinterpret_cast<int64_t *>(p + b_off + b_src);
   double *oxy = reinterpret_cast<double *>(p + b_off + b_src + b_voff);
   int32_t *onv = reinterpret_cast<int32_t *>(p + b_off + b_src + b_voff + b_xy);
-  int32_t *oh = onv + nc;
+  int32_t *oh = reinterpret_cast<int32_t *>(p + b_off + b_src + b_voff + b_xy + b_nv);
   if (n > 0) {
     rc = exclusive_scan<int32_t>(r->pair_ncont, n, off, off + n, s);
   } else {
