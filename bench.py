@@ -611,7 +611,7 @@ def _same(a, b):
     return len(a) == len(b) and all(h1 == h2 and np.array_equal(v1, v2) for (h1, v1), (h2, v2) in zip(a, b))
 
 
-def batched_overlay(prt, scale: float = 1.0, plain_stride: int = 32):
+def batched_overlay(prt, scale: float = 1.0, plain_stride: int = 8):
     """The batched uneven overlay configuration: two layers of `scale` x 1M
     star polygons (vertex count clip(Zipf(1.2), 4, 4096), 5% with 1-3 clockwise
     holes, centres from the 64-Gaussian mixture, radius log-uniform
