@@ -323,16 +323,16 @@ __global__ void td_key32_kernel(const Box<T> *__restrict__ b, const uint32_t *__
   }
 }
 
-// Top-down level with a single run (the first level when one run holds all
-// records), 32-bit coordinates: the key is the coordinate alone.
-template <typename T>
-__global__ void td_key32u_kernel(const Box<T> *__restrict__ b, const uint32_t *__restrict__ perm, int64_t n,
-                                 int use_y, uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+// Top-down level whose runs are sorted one by one (radix_sort_runs) or that
+// is one run: the key is the coordinate's order-preserving image alone.
+template <typename T, typename K>
+__global__ void td_keyrun_kernel(const Box<T> *__restrict__ b, const uint32_t *__restrict__ perm, int64_t n,
+                                 int use_y, K *__restrict__ keys, uint32_t *__restrict__ vals) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     uint32_t r = perm ? perm[i] : (uint32_t)i;
     if ((int64_t)r >= n) r = 0;  // only after a timed-out sort (reported by the caller)
-    Box<T> x = load_box(b, r);
-    keys[i] = ukey(use_y ? x.y1 : x.x1);
+    const T *c = reinterpret_cast<const T *>(b);
+    keys[i] = (K)ukey(__ldg(&c[4 * (int64_t)r + (use_y ? 1 : 0)]));
     vals[i] = r;
   }
 }
@@ -886,22 +886,24 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
         return td_local_level<T>(d_boxes, cur, n, seg, use_y, tmp, s);
       });
       std::swap(perm, tmp);
-    } else if (!wide && seg_bits == 0) {
-      // one run: a stable sort by the 32-bit coordinate alone
-      uint32_t *kk0 = reinterpret_cast<uint32_t *>(k0), *kk1 = reinterpret_cast<uint32_t *>(k1);
+    } else if (seg % kSortRunTile == 0 || seg == n) {
+      // runs of whole sort tiles (or one run): every run sorted on its own by
+      // the coordinate alone, 4 (32-bit) or 8 (64-bit) passes
       rc = dispatch_coord(coord_type, [&](auto tag) {
         using T = decltype(tag);
-        if constexpr (sizeof(T) == 4) {
-          PRT_PROF("td_key32", s);
-          td_key32u_kernel<T><<<g, 256, 0, s>>>(reinterpret_cast<const Box<T> *>(d_boxes), cur, n, use_y, kk0, v0);
+        using K = typename std::conditional<sizeof(T) == 8, uint64_t, uint32_t>::type;
+        K *kk0 = reinterpret_cast<K *>(k0), *kk1 = reinterpret_cast<K *>(k1);
+        {
+          PRT_PROF("td_key", s);
+          td_keyrun_kernel<T, K><<<g, 256, 0, s>>>(reinterpret_cast<const Box<T> *>(d_boxes), cur, n, use_y, kk0, v0);
         }
-        return PRT_OK;
-      });
-      if (!rc) rc = radix_sort_pairs<uint32_t>(kk0, v0, kk1, v1, n, 32, sel, err, s);
-      if (!rc) {
+        int r2 = seg == n ? radix_sort_pairs<K>(kk0, v0, kk1, v1, n, 8 * (int)sizeof(K), sel, err, s)
+                          : radix_sort_runs<K>(kk0, v0, kk1, v1, n, seg, sel, err, s);
+        if (r2) return r2;
         PRT_PROF("select_copy_u32", s);
         select_copy_u32_kernel<<<g, 256, 0, s>>>(v0, v1, sel, n, perm);
-      }
+        return PRT_OK;
+      });
     } else if (!wide) {
       rc = dispatch_coord(coord_type, [&](auto tag) {
         using T = decltype(tag);

@@ -199,6 +199,15 @@ int radix_sort_pairs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1,
                      int key_bits, int *d_sel, unsigned *d_err, cudaStream_t s,
                      const uint32_t *d_hist = nullptr);
 
+// The same sort applied to every run of run_len consecutive pairs
+// independently (all bits of the keys; the last run may be shorter): each run
+// ends sorted in place of itself.  run_len must be a multiple of the sort's
+// 4096-key tile.
+template <typename KeyT>
+int radix_sort_runs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1, int64_t n, int64_t run_len,
+                    int *d_sel, unsigned *d_err, cudaStream_t s);
+constexpr int64_t kSortRunTile = 4096;
+
 // Exclusive prefix sum of n values into d_out (int64); *d_total (device,
 // optional) receives the sum.
 template <typename InT>

@@ -31,6 +31,7 @@ constexpr int kSortWarps = kSortBlock / 32;
 #endif
 constexpr int kItems = PRT_SORT_ITEMS;
 constexpr int kTile = kSortBlock * kItems;
+static_assert(kTile == kSortRunTile, "the run sort's tile");
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kCountMask = (1u << 30) - 1;
@@ -134,7 +135,7 @@ __global__ void __launch_bounds__(kSortBlock, PRT_SORT_MIN_BLOCKS) onesweep_pass
                                                            const PassPlan *__restrict__ plan,
                                                            const uint32_t *__restrict__ goff,
                                                            uint32_t *status, unsigned *tile_ticket,
-                                                           unsigned *err, WaitLimit wl) {
+                                                           unsigned *err, WaitLimit wl, int64_t tiles_per_run) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   PassSmem<KeyT> &S = *reinterpret_cast<PassSmem<KeyT> *>(smem_raw);
   const PassPlan pp = *plan;
@@ -152,6 +153,11 @@ __global__ void __launch_bounds__(kSortBlock, PRT_SORT_MIN_BLOCKS) onesweep_pass
   const int tile = S.tile;
   const int64_t base = (int64_t)tile * kTile;
   const int valid = (int)min((int64_t)kTile, n - base);
+  // runs sorted independently (tiles_per_run > 0): the tile's run, its first
+  // tile and its digit offsets; otherwise one run
+  const int64_t run = tiles_per_run > 0 ? tile / tiles_per_run : 0;
+  const int first = (int)(run * tiles_per_run);
+  goff += run * kRadix;
   const int wb = warp * 32 * kItems;  // this warp's first item in the tile
 
   KeyT k[kItems];
@@ -207,7 +213,7 @@ __global__ void __launch_bounds__(kSortBlock, PRT_SORT_MIN_BLOCKS) onesweep_pass
     total += c;
   }
   uint32_t *st = status + (int64_t)tile * kRadix + d;
-  if (tile == 0) atomicExch(st, kFlagPrefix | ((goff[d] + total) & kCountMask));
+  if (tile == first) atomicExch(st, kFlagPrefix | ((goff[d] + total) & kCountMask));
   else atomicExch(st, kFlagAgg | (total & kCountMask));
   // tile-local exclusive scan over digits: shuffle scan per warp of 32
   // digits, then the 8 warp totals
@@ -239,7 +245,7 @@ __global__ void __launch_bounds__(kSortBlock, PRT_SORT_MIN_BLOCKS) onesweep_pass
   // 4. decoupled look-back for digit d, kLookBatch predecessor statuses per
   //    round trip; every wait is bounded
   uint32_t excl = goff[d];
-  if (tile > 0) {
+  if (tile > first) {  // the run's first tile publishes a prefix: the look-back stops there
     uint32_t acc = 0;
     int t = tile - 1;
     int spins = 0;
@@ -295,7 +301,138 @@ __global__ void __launch_bounds__(kSortBlock, PRT_SORT_MIN_BLOCKS) onesweep_pass
   }
 }
 
+// Digit histograms of every pass per run (runs of tiles_per_run tiles): one
+// block per tile, block histograms in shared memory, one global add per
+// nonzero bin into hist[(run * passes + p) * 256 + digit].
+template <typename KeyT>
+__global__ void __launch_bounds__(256) run_hist_kernel(const KeyT *__restrict__ keys, int64_t n, int passes,
+                                                       int64_t tiles_per_run, uint32_t *__restrict__ hist) {
+  extern __shared__ uint32_t sh[];  // passes * 256
+  for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * kTile;
+  const int64_t end = min(base + (int64_t)kTile, n);
+  for (int64_t i = base + threadIdx.x; i < end; i += blockDim.x) {
+    const KeyT k = keys[i];
+    for (int p = 0; p < passes; p++) atomicAdd(&sh[p * kRadix + (int)((k >> (8 * p)) & 0xFF)], 1u);
+  }
+  __syncthreads();
+  uint32_t *h = hist + (int64_t)(blockIdx.x / tiles_per_run) * passes * kRadix;
+  for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x)
+    if (sh[i]) atomicAdd(&h[i], sh[i]);
+}
+
+// Per run and pass: goff[(p * runs + run) * 256 + d] = the run's first
+// position + the run's exclusive digit scan; trivial[p] is cleared when some
+// run has more than one digit in pass p.  One block (256 threads) per run.
+__global__ void run_plan_kernel(const uint32_t *__restrict__ hist, int64_t n, int64_t run_len, int64_t runs,
+                                int passes, uint32_t *__restrict__ goff, int *__restrict__ trivial) {
+  __shared__ uint32_t scan[kRadix];
+  const int64_t run = blockIdx.x;
+  const int64_t start = run * run_len;
+  const int64_t len = min(run_len, n - start);
+  const int d = threadIdx.x;
+  for (int p = 0; p < passes; p++) {
+    const uint32_t c = hist[(run * passes + p) * kRadix + d];
+    scan[d] = c;
+    __syncthreads();
+    if ((int64_t)c != len && c != 0) trivial[p] = 0;
+    for (int o = 1; o < kRadix; o <<= 1) {
+      const uint32_t v = d >= o ? scan[d - o] : 0u;
+      __syncthreads();
+      scan[d] += v;
+      __syncthreads();
+    }
+    goff[((int64_t)p * runs + run) * kRadix + d] = (uint32_t)start + scan[d] - c;
+    __syncthreads();
+  }
+}
+
+// Pass plans from the trivial flags (a pass whose digit is constant within
+// every run moves nothing and is skipped).
+__global__ void run_plan_final_kernel(const int *__restrict__ trivial, int passes, PassPlan *__restrict__ plan,
+                                      int *__restrict__ d_sel) {
+  int cur = 0;
+  for (int p = 0; p < passes; p++) {
+    PassPlan pp;
+    pp.active = !trivial[p];
+    pp.src = cur;
+    pp.dst = 1 - cur;
+    pp.pad = 0;
+    if (pp.active) cur = 1 - cur;
+    plan[p] = pp;
+  }
+  *d_sel = cur;
+}
+
 }  // namespace
+
+template <typename KeyT>
+int radix_sort_runs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1, int64_t n, int64_t run_len,
+                    int *d_sel, unsigned *d_err, cudaStream_t s) {
+  PRT_CHECK(n >= 0 && n < (int64_t)kCountMask, PRT_ERR_INVALID, "radix sort: n=%lld out of range",
+            (long long)n);
+  PRT_CHECK(run_len >= kTile && run_len % kTile == 0, PRT_ERR_INVALID,
+            "run sort: run length %lld is not a multiple of the %d-key tile", (long long)run_len, kTile);
+  if (n == 0) {
+    PRT_CUDA(cudaMemsetAsync(d_sel, 0, sizeof(int), s));
+    return PRT_OK;
+  }
+  const int passes = (int)sizeof(KeyT);
+  const int64_t tiles = (n + kTile - 1) / kTile;
+  const int64_t tpr = run_len / kTile;
+  const int64_t runs = (n + run_len - 1) / run_len;
+  // scratch: trivial flags, plan, tickets, per-run histograms, per-run offsets, status
+  const size_t triv_b = 64, plan_b = sizeof(PassPlan) * passes, tick_b = 64;
+  const size_t hist_b = sizeof(uint32_t) * (size_t)runs * passes * kRadix;
+  const size_t stat_b = sizeof(uint32_t) * (size_t)tiles * kRadix * passes;
+  unsigned char *scratch = nullptr;
+  const size_t head = 256;  // trivial (64) + plan (<= 128) + tickets (64)
+  size_t total = head + 2 * hist_b + stat_b;
+  int rc = dmalloc(reinterpret_cast<void **>(&scratch), total, s);
+  if (rc) return rc;
+  int *trivial = reinterpret_cast<int *>(scratch);
+  PassPlan *plan = reinterpret_cast<PassPlan *>(scratch + triv_b);
+  unsigned *tick = reinterpret_cast<unsigned *>(scratch + triv_b + 128);
+  uint32_t *hist = reinterpret_cast<uint32_t *>(scratch + head);
+  uint32_t *goff = hist + (size_t)runs * passes * kRadix;
+  uint32_t *status = goff + (size_t)runs * passes * kRadix;
+  (void)plan_b;
+  (void)tick_b;
+  cudaError_t e = cudaMemsetAsync(scratch, 0, total, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(trivial, 0xFF, sizeof(int) * passes, s);  // nonzero = trivial
+  if (e == cudaSuccess) {
+    {
+      PRT_PROF("run_hist", s);
+      run_hist_kernel<KeyT><<<(unsigned)tiles, 256, sizeof(uint32_t) * passes * kRadix, s>>>(keys0, n, passes, tpr,
+                                                                                            hist);
+    }
+    {
+      PRT_PROF("plan", s);
+      run_plan_kernel<<<(unsigned)runs, kRadix, 0, s>>>(hist, n, run_len, runs, passes, goff, trivial);
+      run_plan_final_kernel<<<1, 1, 0, s>>>(trivial, passes, plan, d_sel);
+    }
+    size_t smem = sizeof(PassSmem<KeyT>);
+    static bool attr_done[256] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 256 || !attr_done[dev]) {
+      e = cudaFuncSetAttribute(onesweep_pass<KeyT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess && dev >= 0 && dev < 256) attr_done[dev] = true;
+    }
+    const WaitLimit wl = wait_limit();
+    for (int p = 0; p < passes && e == cudaSuccess; p++) {
+      PRT_PROF("onesweep_pass", s);
+      onesweep_pass<KeyT><<<(unsigned)tiles, kSortBlock, smem, s>>>(
+        keys0, vals0, keys1, vals1, n, 8 * p, plan + p, goff + (size_t)p * runs * kRadix,
+        status + (size_t)p * tiles * kRadix, tick + p, d_err, wl, tpr);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+  }
+  dfree(scratch, s);
+  if (e != cudaSuccess) return cuda_status(e, "radix_sort_runs");
+  return PRT_OK;
+}
 
 template <typename KeyT>
 int radix_sort_pairs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1, int64_t n, int key_bits,
@@ -351,7 +488,7 @@ int radix_sort_pairs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1,
         PRT_PROF("onesweep_pass", s);
         onesweep_pass<KeyT><<<(unsigned)tiles, kSortBlock, smem, s>>>(
           keys0, vals0, keys1, vals1, n, 8 * p, plan + p, goff + p * kRadix,
-          status + (size_t)p * tiles * kRadix, tick + p, d_err, wl);
+          status + (size_t)p * tiles * kRadix, tick + p, d_err, wl, 0);
       }
     }
     if (e == cudaSuccess) e = cudaGetLastError();
@@ -368,6 +505,10 @@ std::atomic<int> g_wait_blind{0};
 
 WaitLimit wait_limit() { return WaitLimit{g_wait_polls.load(), g_wait_blind.load()}; }
 
+template int radix_sort_runs<uint32_t>(uint32_t *, uint32_t *, uint32_t *, uint32_t *, int64_t, int64_t, int *,
+                                       unsigned *, cudaStream_t);
+template int radix_sort_runs<uint64_t>(uint64_t *, uint32_t *, uint64_t *, uint32_t *, int64_t, int64_t, int *,
+                                       unsigned *, cudaStream_t);
 template int radix_sort_pairs<uint32_t>(uint32_t *, uint32_t *, uint32_t *, uint32_t *, int64_t, int, int *,
                                         unsigned *, cudaStream_t, const uint32_t *);
 template int radix_sort_pairs<uint64_t>(uint64_t *, uint32_t *, uint64_t *, uint32_t *, int64_t, int, int *,
