@@ -482,53 +482,44 @@ __device__ inline bool pair_boundary(const BwdPoly *M, const float4 *ext, int na
     if (valid && !exact) {
       const double rl = fabs(rx) + fabs(ry);
       const int s0 = g(pb.y), s1 = g(pb.w), x0 = gx(pb.x), x1 = gx(pb.z);
-      // one candidate edge k of Q against this lane's edge
-      auto test = [&](int k, const float4 &b) {
-        if (b.w < pb.y || b.y > pb.w || b.z < pb.x || b.x > pb.z) return;
-        const int l = Q.nxt[k];
-        const double ax = Q.x[k], ay = Q.y[k], bx = Q.x[l], by = Q.y[l];
-        const double sx = bx - ax, sy = by - ay;
-        const double den = rx * sy - ry * sx;
-        const double apx = ax - px, apy = ay - py;
-        const double tn = apx * sy - apy * sx;
-        if (den == 0.0) {
-          unclean |= tn == 0.0;  // collinear
-          return;
-        }
-        const double un = apx * ry - apy * rx;
-        // t = tn / den and u = un / den, with the signs of den folded in
-        const double d = fabs(den), tol = 1e-9 * d;
-        const double tt = den > 0.0 ? tn : -tn, uu = den > 0.0 ? un : -un;
-        if (tt < -tol || tt > d + tol || uu < -tol || uu > d + tol) return;  // next_crossing rejects it
-        if (!(tt > tol && tt < d - tol && uu > tol && uu < d - tol && d > 1e-6 * rl * (fabs(sx) + fabs(sy))) ||
-            m == kBwdFast) {
-          unclean = true;
-          return;
-        }
-        if constexpr (kArea) {
-          const double sl = fabs(sx) + fabs(sy);
-          err += (rl + sl) * rl * sl / d;
-        }
-        double v = tn / den;  // next_crossing's t
-        // sorted insert into the register list
-        if (v < t0c) { const double x = t0c; t0c = v; v = x; }
-        if (v < t1c) { const double x = t1c; t1c = v; v = x; }
-        if (v < t2c) { const double x = t2c; t2c = v; v = x; }
-        if (v < t3c) { const double x = t3c; t3c = v; v = x; }
-        m++;
-      };
       for (int c = 0; c < nwq; c++) {
         uint32_t bits = bwd_cands(Q, c, s0, s1, x0, x1);
-        // two candidates per step: both boxes are read before either test
         while (bits) {
-          const int k0 = 32 * c + __ffs(bits) - 1;
+          const int k = 32 * c + __ffs(bits) - 1;
           bits &= bits - 1;
-          const bool two = bits != 0;
-          const int k1 = two ? 32 * c + __ffs(bits) - 1 : k0;
-          if (two) bits &= bits - 1;
-          const float4 b0 = Q.bb[k0], b1 = Q.bb[k1];
-          test(k0, b0);
-          if (two) test(k1, b1);
+          const float4 b = Q.bb[k];
+          if (b.w < pb.y || b.y > pb.w || b.z < pb.x || b.x > pb.z) continue;
+          const int l = Q.nxt[k];
+          const double ax = Q.x[k], ay = Q.y[k], bx = Q.x[l], by = Q.y[l];
+          const double sx = bx - ax, sy = by - ay;
+          const double den = rx * sy - ry * sx;
+          const double apx = ax - px, apy = ay - py;
+          const double tn = apx * sy - apy * sx;
+          if (den == 0.0) {
+            unclean |= tn == 0.0;  // collinear
+            continue;
+          }
+          const double un = apx * ry - apy * rx;
+          // t = tn / den and u = un / den, with the signs of den folded in
+          const double d = fabs(den), tol = 1e-9 * d;
+          const double tt = den > 0.0 ? tn : -tn, uu = den > 0.0 ? un : -un;
+          if (tt < -tol || tt > d + tol || uu < -tol || uu > d + tol) continue;  // next_crossing rejects it
+          if (!(tt > tol && tt < d - tol && uu > tol && uu < d - tol && d > 1e-6 * rl * (fabs(sx) + fabs(sy))) ||
+              m == kBwdFast) {
+            unclean = true;
+            continue;
+          }
+          if constexpr (kArea) {
+            const double sl = fabs(sx) + fabs(sy);
+            err += (rl + sl) * rl * sl / d;
+          }
+          double v = (apx * sy - apy * sx) / den;  // next_crossing's t
+          // sorted insert into the register list
+          if (v < t0c) { const double x = t0c; t0c = v; v = x; }
+          if (v < t1c) { const double x = t1c; t1c = v; v = x; }
+          if (v < t2c) { const double x = t2c; t2c = v; v = x; }
+          if (v < t3c) { const double x = t3c; t3c = v; v = x; }
+          m++;
         }
       }
       unclean |= (m > 1 && t0c == t1c) || (m > 2 && t1c == t2c) || (m > 3 && t2c == t3c);

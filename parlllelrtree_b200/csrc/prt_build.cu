@@ -375,17 +375,22 @@ __global__ void select_copy_u32_kernel(const uint32_t *a, const uint32_t *b, con
 
 // ------------------------------------------------------------------ top-down, short runs
 
-// A top-down level whose runs hold at most kTdLocal records is sorted run by
-// run in shared memory: one CTA takes as many whole runs as fit in a tile of
-// kTdLocal records (in the current order), gathers each record's coordinate
-// key, and sorts the tile stably by (run within the tile, key) with an LSD
-// radix sort in shared memory, 8 bits per pass, each pass ranked by the warp
-// multisplit (lanes with the same digit from one ballot per digit bit).  The
-// tile's index order is the current order, so equal keys keep it, as the
-// level's stable sort requires.  This replaces 4-7 global passes over 64-bit
-// keys by one gather, one read and one write of the order.
+// The top-down levels whose runs hold at most kTdLocal records (the last
+// levels of the build: run lengths F^k <= 4096, each dividing the one before)
+// are sorted together, tile by tile, in shared memory: one CTA takes as many
+// whole runs of the first such level as fit in a tile of kTdLocal records (in
+// the current order), and for each level in turn gathers each record's
+// coordinate key (the first level's gather leaves the tile's boxes in L2 for
+// the later ones) and sorts the tile stably by (run within the tile, key)
+// with an LSD radix sort in shared memory, 8 bits per pass, each pass ranked
+// by the warp multisplit (lanes with the same digit from one ballot per digit
+// bit).  The tile's index order is the current order, so equal keys keep it,
+// as each level's stable sort requires; each item's run is carried along the
+// passes.  One read and one write of the order replace 4-7 global passes per
+// level.
 constexpr int kTdLocal = 4096;
 constexpr int kTdItems = kTdLocal / 256;  // per thread (256 threads)
+constexpr int kTdMaxLocal = 12;           // local levels one launch sorts (4096 = 2^12)
 
 __device__ __forceinline__ uint32_t lane_lt() {
   uint32_t m;
@@ -403,113 +408,128 @@ struct TdLocalSmem {
   uint32_t wsum[8];
 };
 
+// The local levels, in order: run length and axis (0: x1, 1: y1) of each.
+struct TdLocalLevels {
+  int64_t seg[kTdMaxLocal];
+  int use_y[kTdMaxLocal];
+  int count;
+};
+
 template <typename T, typename K>
 __global__ void __launch_bounds__(256) td_local_sort_kernel(const Box<T> *__restrict__ b,
                                                             const uint32_t *__restrict__ perm_in, int64_t n,
-                                                            int64_t seg, int use_y, int run_bits,
-                                                            uint32_t *__restrict__ perm_out) {
+                                                            TdLocalLevels lv, uint32_t *__restrict__ perm_out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TdLocalSmem<K> &S = *reinterpret_cast<TdLocalSmem<K> *>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int64_t chunk = (kTdLocal / seg) * seg;  // whole runs per tile
+  const int64_t chunk = (kTdLocal / lv.seg[0]) * lv.seg[0];  // whole runs of the first local level
   const int64_t base = blockIdx.x * chunk;
   const int m = (int)min(chunk, n - base);
   constexpr int kKeyBits = 8 * (int)sizeof(K);
   const T *c = reinterpret_cast<const T *>(b);
-  // keys: (run within the tile) above the coordinate's order-preserving image
   for (int i = tid; i < m; i += 256) {
     uint32_t r = perm_in ? perm_in[base + i] : (uint32_t)(base + i);
     if ((int64_t)r >= n) r = 0;  // only after a timed-out sort (reported by the caller)
-    const T v = __ldg(&c[4 * (int64_t)r + (use_y ? 1 : 0)]);
-    S.key[0][i] = (K)ukey(v);
     S.val[0][i] = r;
-    S.run[0][i] = (uint16_t)(i / seg);
   }
-  __syncthreads();
-  const int total_bits = kKeyBits + run_bits;
   const uint32_t lt = lane_lt();
   int cur = 0;
-  for (int shift = 0; shift < total_bits; shift += 8) {
-    for (int i = tid; i < 8 * 256; i += 256) (&S.wh[0][0])[i] = 0;
+  for (int level = 0; level < lv.count; level++) {
+    const int64_t seg = lv.seg[level];
+    const int axis = lv.use_y[level];
+    int run_bits = 0;
+    while ((1ll << run_bits) < kTdLocal / seg) run_bits++;
     __syncthreads();
-    // digit of the item at position i: the key's byte, or above the key the
-    // run index (positions change from pass to pass; the run moves along)
-    auto digit = [&](int i) -> int {
-      if (shift < kKeyBits) return (int)((S.key[cur][i] >> shift) & 0xFF);
-      return (int)((S.run[cur][i] >> (shift - kKeyBits)) & 0xFF);
-    };
-    int dg[kTdItems];
-    uint32_t rk[kTdItems];
-    uint32_t *wh = S.wh[warp];
+    // keys: the coordinate's order-preserving image, and the run (in the
+    // order the previous level left) above it
+    for (int i = tid; i < m; i += 256) {
+      const T v = __ldg(&c[4 * (int64_t)S.val[cur][i] + axis]);
+      S.key[cur][i] = (K)ukey(v);
+      S.run[cur][i] = (uint16_t)(i / seg);
+    }
+    const int total_bits = kKeyBits + run_bits;
+    for (int shift = 0; shift < total_bits; shift += 8) {
+      __syncthreads();
+      for (int i = tid; i < 8 * 256; i += 256) (&S.wh[0][0])[i] = 0;
+      __syncthreads();
+      // digit of the item at position i: the key's byte, or above the key
+      // the run index (positions change from pass to pass; the run moves along)
+      auto digit = [&](int i) -> int {
+        if (shift < kKeyBits) return (int)((S.key[cur][i] >> shift) & 0xFF);
+        return (int)((S.run[cur][i] >> (shift - kKeyBits)) & 0xFF);
+      };
+      int dg[kTdItems];
+      uint32_t rk[kTdItems];
+      uint32_t *wh = S.wh[warp];
 #pragma unroll
-    for (int j = 0; j < kTdItems; j++) {
-      const int i = warp * (32 * kTdItems) + j * 32 + lane;
-      const bool ok = i < m;
-      const int d = ok ? digit(i) : 256 + lane;
-      uint32_t peers = __ballot_sync(0xffffffffu, ok);
+      for (int j = 0; j < kTdItems; j++) {
+        const int i = warp * (32 * kTdItems) + j * 32 + lane;
+        const bool ok = i < m;
+        const int d = ok ? digit(i) : 256 + lane;
+        uint32_t peers = __ballot_sync(0xffffffffu, ok);
 #pragma unroll
-      for (int bit = 0; bit < 8; bit++) {
-        const uint32_t bm = __ballot_sync(0xffffffffu, (d >> bit) & 1);
-        peers &= ((d >> bit) & 1) ? bm : ~bm;
+        for (int bit = 0; bit < 8; bit++) {
+          const uint32_t bm = __ballot_sync(0xffffffffu, (d >> bit) & 1);
+          peers &= ((d >> bit) & 1) ? bm : ~bm;
+        }
+        if (!ok) peers = 1u << lane;
+        const int leader = __ffs(peers) - 1;
+        uint32_t cnt = 0;
+        if (lane == leader && ok) {
+          cnt = wh[d];
+          wh[d] = cnt + __popc(peers);
+        }
+        cnt = __shfl_sync(0xffffffffu, cnt, leader);
+        dg[j] = d;
+        rk[j] = cnt + __popc(peers & lt);
+        __syncwarp();
       }
-      if (!ok) peers = 1u << lane;
-      const int leader = __ffs(peers) - 1;
-      uint32_t cnt = 0;
-      if (lane == leader && ok) {
-        cnt = wh[d];
-        wh[d] = cnt + __popc(peers);
+      __syncthreads();
+      // thread d: exclusive prefix of digit d over the warps, then over digits
+      uint32_t tot = 0;
+#pragma unroll
+      for (int w = 0; w < 8; w++) {
+        const uint32_t x = S.wh[w][tid];
+        S.wh[w][tid] = tot;
+        tot += x;
       }
-      cnt = __shfl_sync(0xffffffffu, cnt, leader);
-      dg[j] = d;
-      rk[j] = cnt + __popc(peers & lt);
-      __syncwarp();
-    }
-    __syncthreads();
-    // thread d: exclusive prefix of digit d over the warps, then over digits
-    uint32_t tot = 0;
+      uint32_t incl = tot;
 #pragma unroll
-    for (int w = 0; w < 8; w++) {
-      const uint32_t x = S.wh[w][tid];
-      S.wh[w][tid] = tot;
-      tot += x;
-    }
-    uint32_t incl = tot;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += y;
-    }
-    if (lane == 31) S.wsum[warp] = incl;
-    __syncthreads();
-    uint32_t woff = 0;
-#pragma unroll
-    for (int w = 0; w < 8; w++) woff += w < warp ? S.wsum[w] : 0u;
-    S.dstart[tid] = woff + incl - tot;
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < kTdItems; j++) {
-      const int i = warp * (32 * kTdItems) + j * 32 + lane;
-      if (i < m) {
-        const uint32_t pos = S.dstart[dg[j]] + S.wh[warp][dg[j]] + rk[j];
-        S.key[1 - cur][pos] = S.key[cur][i];
-        S.val[1 - cur][pos] = S.val[cur][i];
-        S.run[1 - cur][pos] = S.run[cur][i];
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
       }
+      if (lane == 31) S.wsum[warp] = incl;
+      __syncthreads();
+      uint32_t woff = 0;
+#pragma unroll
+      for (int w = 0; w < 8; w++) woff += w < warp ? S.wsum[w] : 0u;
+      S.dstart[tid] = woff + incl - tot;
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < kTdItems; j++) {
+        const int i = warp * (32 * kTdItems) + j * 32 + lane;
+        if (i < m) {
+          const uint32_t pos = S.dstart[dg[j]] + S.wh[warp][dg[j]] + rk[j];
+          S.key[1 - cur][pos] = S.key[cur][i];
+          S.val[1 - cur][pos] = S.val[cur][i];
+          S.run[1 - cur][pos] = S.run[cur][i];
+        }
+      }
+      cur = 1 - cur;
     }
-    cur = 1 - cur;
-    __syncthreads();
   }
+  __syncthreads();
   for (int i = tid; i < m; i += 256) perm_out[base + i] = S.val[cur][i];
 }
 
-// Launches the short-run sort of one top-down level (seg <= kTdLocal).
+// Launches the short-run sort of the local levels lv (first run length at
+// most kTdLocal, each next one dividing it).
 template <typename T>
-int td_local_level(const void *d_boxes, const uint32_t *perm_in, int64_t n, int64_t seg, int use_y,
-                   uint32_t *perm_out, cudaStream_t s) {
+int td_local_levels(const void *d_boxes, const uint32_t *perm_in, int64_t n, const TdLocalLevels &lv,
+                    uint32_t *perm_out, cudaStream_t s) {
   using K = typename std::conditional<sizeof(T) == 8, uint64_t, uint32_t>::type;
-  const int64_t chunk = (kTdLocal / seg) * seg;
-  int run_bits = 0;
-  while ((1ll << run_bits) < kTdLocal / seg) run_bits++;
+  const int64_t chunk = (kTdLocal / lv.seg[0]) * lv.seg[0];
   const size_t smem = sizeof(TdLocalSmem<K>);
   static bool attr_done[256] = {false};
   int dev = 0;
@@ -523,7 +543,7 @@ int td_local_level(const void *d_boxes, const uint32_t *perm_in, int64_t n, int6
   {
     PRT_PROF("td_local_sort", s);
     td_local_sort_kernel<T, K><<<(unsigned)blocks, 256, smem, s>>>(reinterpret_cast<const Box<T> *>(d_boxes),
-                                                                   perm_in, n, seg, use_y, run_bits, perm_out);
+                                                                   perm_in, n, lv, perm_out);
   }
   PRT_CUDA(cudaGetLastError());
   return PRT_OK;
@@ -880,12 +900,26 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
     const int use_y = p & 1;
     const uint32_t *cur = have_perm ? perm : nullptr;
     if (seg <= kTdLocal) {
-      // short runs: sorted run by run in shared memory, into tmp
+      // this and every later level have short runs: all of them sorted in
+      // shared memory by one launch, into tmp
+      TdLocalLevels lv;
+      lv.count = 0;
+      for (int q = p; q < H && lv.count < kTdMaxLocal; q++) {
+        // run length fanout^(H-q), saturated at n like seg (only when all n
+        // records fit in one tile)
+        int64_t sq = 1;
+        for (int k = 0; k < H - q && sq < n; k++) sq *= fanout;
+        if (sq > n) sq = n;
+        lv.seg[lv.count] = sq;
+        lv.use_y[lv.count] = q & 1;
+        lv.count++;
+      }
       rc = dispatch_coord(coord_type, [&](auto tag) {
         using T = decltype(tag);
-        return td_local_level<T>(d_boxes, cur, n, seg, use_y, tmp, s);
+        return td_local_levels<T>(d_boxes, cur, n, lv, tmp, s);
       });
       std::swap(perm, tmp);
+      p += lv.count - 1;  // the loop's p++ moves past the last local level
     } else if (seg % kSortRunTile == 0 || seg == n) {
       // runs of whole sort tiles (or one run): every run sorted on its own by
       // the coordinate alone, 4 (32-bit) or 8 (64-bit) passes
