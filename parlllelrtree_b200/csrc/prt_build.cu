@@ -323,18 +323,58 @@ __global__ void td_key32_kernel(const Box<T> *__restrict__ b, const uint32_t *__
   }
 }
 
+// The current top-down order: perm_a or perm_b as *sel says (sel nullptr:
+// perm_a; perm_a nullptr: the identity).
+__device__ __forceinline__ const uint32_t *cur_perm(const uint32_t *perm_a, const uint32_t *perm_b, const int *sel) {
+  return perm_a ? ((sel && *sel) ? perm_b : perm_a) : nullptr;
+}
+
 // Top-down level whose runs are sorted one by one (radix_sort_runs) or that
-// is one run: the key is the coordinate's order-preserving image alone.
+// is one run: the key is the coordinate's order-preserving image alone.  One
+// block per 4096 positions (inside one run, since runs are whole tiles)
+// counts the digit histograms of every pass on the way, into its run's
+// histograms hist[(run * passes + p) * 256 + digit], so the sort does not
+// read the keys again to count them.  The order is read and the values
+// written at the same positions by the same thread: vals may be the buffer
+// the order is read from.
 template <typename T, typename K>
-__global__ void td_keyrun_kernel(const Box<T> *__restrict__ b, const uint32_t *__restrict__ perm, int64_t n,
-                                 int use_y, K *__restrict__ keys, uint32_t *__restrict__ vals) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    uint32_t r = perm ? perm[i] : (uint32_t)i;
-    if ((int64_t)r >= n) r = 0;  // only after a timed-out sort (reported by the caller)
-    const T *c = reinterpret_cast<const T *>(b);
-    keys[i] = (K)ukey(__ldg(&c[4 * (int64_t)r + (use_y ? 1 : 0)]));
-    vals[i] = r;
+__global__ void __launch_bounds__(256) td_keyrun_kernel(const Box<T> *__restrict__ b, const uint32_t *perm_a,
+                                                        const uint32_t *perm_b, const int *sel, int64_t n, int use_y,
+                                                        int64_t tiles_per_run, K *__restrict__ keys, uint32_t *vals,
+                                                        uint32_t *__restrict__ hist) {
+  constexpr int kPasses = (int)sizeof(K);
+  constexpr int kPer = (int)(kSortRunTile / 256);
+  __shared__ uint32_t sh[kPasses * 256];
+  for (int i = threadIdx.x; i < kPasses * 256; i += 256) sh[i] = 0;
+  __syncthreads();
+  const uint32_t *perm = cur_perm(perm_a, perm_b, sel);
+  const T *c = reinterpret_cast<const T *>(b) + (use_y ? 1 : 0);
+  const int64_t base = (int64_t)blockIdx.x * kSortRunTile + threadIdx.x;
+  // all loads of the order first, then all coordinate loads, then the stores
+  uint32_t r[kPer];
+#pragma unroll
+  for (int j = 0; j < kPer; j++) {
+    const int64_t i = base + 256 * j;
+    r[j] = i < n ? (perm ? perm[i] : (uint32_t)i) : 0u;
+    if ((int64_t)r[j] >= n) r[j] = 0;  // only after a timed-out sort (reported by the caller)
   }
+  K k[kPer];
+#pragma unroll
+  for (int j = 0; j < kPer; j++) k[j] = base + 256 * j < n ? (K)ukey(__ldg(&c[4 * (int64_t)r[j]])) : K(0);
+#pragma unroll
+  for (int j = 0; j < kPer; j++) {
+    const int64_t i = base + 256 * j;
+    if (i < n) {
+      keys[i] = k[j];
+      vals[i] = r[j];
+#pragma unroll
+      for (int p = 0; p < kPasses; p++) atomicAdd(&sh[p * 256 + (int)((k[j] >> (8 * p)) & 0xFF)], 1u);
+    }
+  }
+  __syncthreads();
+  uint32_t *h = hist + (int64_t)(blockIdx.x / tiles_per_run) * kPasses * 256;
+  for (int i = threadIdx.x; i < kPasses * 256; i += 256)
+    if (sh[i]) atomicAdd(&h[i], sh[i]);
 }
 
 // Top-down level, 64-bit coordinates, first stage: key = coordinate, value = position.
@@ -398,14 +438,18 @@ __device__ __forceinline__ uint32_t lane_lt() {
   return m;
 }
 
-template <typename K>
+// Shared memory of one tile: the items in the current order (run << 16 |
+// slot, double-buffered; slot = the item's position in the tile's input
+// order), the (x1, y1) of every slot, gathered once for all levels, and the
+// ranking scratch.
+template <typename T>
 struct TdLocalSmem {
-  K key[2][kTdLocal];
-  uint32_t val[2][kTdLocal];
-  uint16_t run[2][kTdLocal];  // run within the tile, moved with its item
+  uint32_t item[2][kTdLocal];
+  T xy[kTdLocal][2];
   uint32_t wh[8][256];
   uint32_t dstart[256];
   uint32_t wsum[8];
+  unsigned long long red[2][8];
 };
 
 // The local levels, in order: run length and axis (0: x1, 1: y1) of each.
@@ -415,49 +459,76 @@ struct TdLocalLevels {
   int count;
 };
 
-template <typename T, typename K>
-__global__ void __launch_bounds__(256) td_local_sort_kernel(const Box<T> *__restrict__ b,
-                                                            const uint32_t *__restrict__ perm_in, int64_t n,
-                                                            TdLocalLevels lv, uint32_t *__restrict__ perm_out) {
+__device__ __forceinline__ int bit_length(uint32_t x) { return 32 - __clz(x); }
+__device__ __forceinline__ int bit_length(uint64_t x) { return 64 - __clzll((long long)x); }
+
+// Each level sorts the tile stably by (run, key - the tile's smallest key):
+// only the bits that difference needs, with the run index directly above
+// them, in 8-bit digits (the last one narrower).  Subtracting one constant
+// from every key keeps their order, so this is the order of a stable sort by
+// key within each run.
+template <typename T>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) td_local_sort_kernel(
+    const Box<T> *__restrict__ b, const uint32_t *__restrict__ perm_a, const uint32_t *__restrict__ perm_b,
+    const int *__restrict__ sel, int64_t n, TdLocalLevels lv, uint32_t *__restrict__ perm_out) {
+  using K = typename std::conditional<sizeof(T) == 8, uint64_t, uint32_t>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  TdLocalSmem<K> &S = *reinterpret_cast<TdLocalSmem<K> *>(smem_raw);
+  TdLocalSmem<T> &S = *reinterpret_cast<TdLocalSmem<T> *>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t chunk = (kTdLocal / lv.seg[0]) * lv.seg[0];  // whole runs of the first local level
   const int64_t base = blockIdx.x * chunk;
   const int m = (int)min(chunk, n - base);
-  constexpr int kKeyBits = 8 * (int)sizeof(K);
   const T *c = reinterpret_cast<const T *>(b);
+  const uint32_t *perm_in = cur_perm(perm_a, perm_b, sel);
   for (int i = tid; i < m; i += 256) {
     uint32_t r = perm_in ? perm_in[base + i] : (uint32_t)(base + i);
     if ((int64_t)r >= n) r = 0;  // only after a timed-out sort (reported by the caller)
-    S.val[0][i] = r;
+    S.xy[i][0] = __ldg(&c[4 * (int64_t)r]);
+    S.xy[i][1] = __ldg(&c[4 * (int64_t)r + 1]);
+    S.item[0][i] = (uint32_t)i;
   }
   const uint32_t lt = lane_lt();
   int cur = 0;
   for (int level = 0; level < lv.count; level++) {
-    const int64_t seg = lv.seg[level];
+    const int seg = (int)min(lv.seg[level], (int64_t)kTdLocal);
     const int axis = lv.use_y[level];
-    int run_bits = 0;
-    while ((1ll << run_bits) < kTdLocal / seg) run_bits++;
     __syncthreads();
-    // keys: the coordinate's order-preserving image, and the run (in the
-    // order the previous level left) above it
+    // the run of each item from its position in the order the previous level
+    // left, and the tile's key range
+    K lo = ~K(0), hi = 0;
     for (int i = tid; i < m; i += 256) {
-      const T v = __ldg(&c[4 * (int64_t)S.val[cur][i] + axis]);
-      S.key[cur][i] = (K)ukey(v);
-      S.run[cur][i] = (uint16_t)(i / seg);
+      const uint32_t slot = S.item[cur][i] & 0xFFFFu;
+      S.item[cur][i] = (uint32_t)(i / seg) << 16 | slot;
+      const K k = (K)ukey(S.xy[slot][axis]);
+      lo = k < lo ? k : lo;
+      hi = k > hi ? k : hi;
     }
-    const int total_bits = kKeyBits + run_bits;
+    for (int o = 16; o; o >>= 1) {
+      const K a = __shfl_xor_sync(0xffffffffu, lo, o), z = __shfl_xor_sync(0xffffffffu, hi, o);
+      lo = a < lo ? a : lo;
+      hi = z > hi ? z : hi;
+    }
+    if (lane == 0) {
+      S.red[0][warp] = lo;
+      S.red[1][warp] = hi;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int w = 0; w < 8; w++) {
+      const K a = (K)S.red[0][w], z = (K)S.red[1][w];
+      lo = a < lo ? a : lo;
+      hi = z > hi ? z : hi;
+    }
+    const int key_bits = hi > lo ? bit_length(hi - lo) : 0;
+    int run_bits = 0;
+    while ((1 << run_bits) < (m + seg - 1) / seg) run_bits++;
+    const int total_bits = key_bits + run_bits;
     for (int shift = 0; shift < total_bits; shift += 8) {
+      const int width = min(8, total_bits - shift);
       __syncthreads();
       for (int i = tid; i < 8 * 256; i += 256) (&S.wh[0][0])[i] = 0;
       __syncthreads();
-      // digit of the item at position i: the key's byte, or above the key
-      // the run index (positions change from pass to pass; the run moves along)
-      auto digit = [&](int i) -> int {
-        if (shift < kKeyBits) return (int)((S.key[cur][i] >> shift) & 0xFF);
-        return (int)((S.run[cur][i] >> (shift - kKeyBits)) & 0xFF);
-      };
+      uint32_t it[kTdItems];
       int dg[kTdItems];
       uint32_t rk[kTdItems];
       uint32_t *wh = S.wh[warp];
@@ -465,12 +536,30 @@ __global__ void __launch_bounds__(256) td_local_sort_kernel(const Box<T> *__rest
       for (int j = 0; j < kTdItems; j++) {
         const int i = warp * (32 * kTdItems) + j * 32 + lane;
         const bool ok = i < m;
-        const int d = ok ? digit(i) : 256 + lane;
+        int d = 256 + lane;
+        it[j] = 0;
+        if (ok) {
+          // digit: bits [shift, shift + width) of (run << key_bits | key - lo)
+          const uint32_t x = S.item[cur][i];
+          const uint32_t run = x >> 16;
+          const K rel = (K)ukey(S.xy[x & 0xFFFFu][axis]) - lo;
+          uint32_t v;
+          if (shift < key_bits) {
+            v = (uint32_t)(rel >> shift);
+            if (shift + 8 > key_bits) v |= run << (key_bits - shift);
+          } else {
+            v = run >> (shift - key_bits);
+          }
+          d = (int)(v & ((1u << width) - 1u));
+          it[j] = x;
+        }
         uint32_t peers = __ballot_sync(0xffffffffu, ok);
 #pragma unroll
         for (int bit = 0; bit < 8; bit++) {
-          const uint32_t bm = __ballot_sync(0xffffffffu, (d >> bit) & 1);
-          peers &= ((d >> bit) & 1) ? bm : ~bm;
+          if (bit < width) {
+            const uint32_t bm = __ballot_sync(0xffffffffu, (d >> bit) & 1);
+            peers &= ((d >> bit) & 1) ? bm : ~bm;
+          }
         }
         if (!ok) peers = 1u << lane;
         const int leader = __ffs(peers) - 1;
@@ -509,41 +598,39 @@ __global__ void __launch_bounds__(256) td_local_sort_kernel(const Box<T> *__rest
 #pragma unroll
       for (int j = 0; j < kTdItems; j++) {
         const int i = warp * (32 * kTdItems) + j * 32 + lane;
-        if (i < m) {
-          const uint32_t pos = S.dstart[dg[j]] + S.wh[warp][dg[j]] + rk[j];
-          S.key[1 - cur][pos] = S.key[cur][i];
-          S.val[1 - cur][pos] = S.val[cur][i];
-          S.run[1 - cur][pos] = S.run[cur][i];
-        }
+        if (i < m) S.item[1 - cur][S.dstart[dg[j]] + S.wh[warp][dg[j]] + rk[j]] = it[j];
       }
       cur = 1 - cur;
     }
   }
   __syncthreads();
-  for (int i = tid; i < m; i += 256) perm_out[base + i] = S.val[cur][i];
+  for (int i = tid; i < m; i += 256) {
+    const uint32_t slot = S.item[cur][i] & 0xFFFFu;
+    uint32_t r = perm_in ? perm_in[base + slot] : (uint32_t)(base + slot);
+    if ((int64_t)r >= n) r = 0;
+    perm_out[base + i] = r;
+  }
 }
 
 // Launches the short-run sort of the local levels lv (first run length at
 // most kTdLocal, each next one dividing it).
 template <typename T>
-int td_local_levels(const void *d_boxes, const uint32_t *perm_in, int64_t n, const TdLocalLevels &lv,
-                    uint32_t *perm_out, cudaStream_t s) {
-  using K = typename std::conditional<sizeof(T) == 8, uint64_t, uint32_t>::type;
+int td_local_levels(const void *d_boxes, const uint32_t *perm_a, const uint32_t *perm_b, const int *sel, int64_t n,
+                    const TdLocalLevels &lv, uint32_t *perm_out, cudaStream_t s) {
   const int64_t chunk = (kTdLocal / lv.seg[0]) * lv.seg[0];
-  const size_t smem = sizeof(TdLocalSmem<K>);
+  const size_t smem = sizeof(TdLocalSmem<T>);
   static bool attr_done[256] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 256 || !attr_done[dev]) {
-    PRT_CUDA(cudaFuncSetAttribute(td_local_sort_kernel<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+    PRT_CUDA(cudaFuncSetAttribute(td_local_sort_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (dev >= 0 && dev < 256) attr_done[dev] = true;
   }
   const int64_t blocks = (n + chunk - 1) / chunk;
   {
     PRT_PROF("td_local_sort", s);
-    td_local_sort_kernel<T, K><<<(unsigned)blocks, 256, smem, s>>>(reinterpret_cast<const Box<T> *>(d_boxes),
-                                                                   perm_in, n, lv, perm_out);
+    td_local_sort_kernel<T><<<(unsigned)blocks, 256, smem, s>>>(reinterpret_cast<const Box<T> *>(d_boxes), perm_a,
+                                                                perm_b, sel, n, lv, perm_out);
   }
   PRT_CUDA(cudaGetLastError());
   return PRT_OK;
@@ -866,7 +953,9 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
   const int H = t->lv.levels;
   const bool wide = coord_size(coord_type) == 8;
   unsigned char *scr = nullptr;
-  size_t need = 64 + 2 * 8 * n + 4 * 4 * n + 64;
+  // per-run digit histograms: at most one run per sort tile, 8 passes
+  const size_t hist_words = (size_t)((n + kSortRunTile - 1) / kSortRunTile) * 8 * 256;
+  size_t need = 64 + 2 * 8 * n + 4 * 4 * n + 4 * hist_words + 64;
   rc = dmalloc(reinterpret_cast<void **>(&scr), need, s);
   if (rc) {
     prt_tree_free(t);
@@ -878,12 +967,26 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
   uint64_t *k1 = k0 + n;
   uint32_t *v0 = reinterpret_cast<uint32_t *>(k1 + n);
   uint32_t *v1 = v0 + n;
-  uint32_t *perm = v1 + n;   // current leaf order
+  uint32_t *perm = v1 + n;  // current leaf order (when materialised)
   uint32_t *tmp = perm + n;  // scratch
+  uint32_t *hist = tmp + n;
   cudaError_t e = cudaMemsetAsync(err, 0, 8, s);
   if (e != cudaSuccess) rc = cuda_status(e, "memset");
   const int g = grid_for(n, 256, 16);
-  bool have_perm = false;
+  // the current order: pa or pb as *psel says (psel nullptr: pa; pa nullptr:
+  // the identity).  A sort leaves it in (v0, v1, sel) and the next level
+  // reads it there; paths that need one array copy it into perm first.
+  const uint32_t *pa = nullptr, *pb = nullptr;
+  const int *psel = nullptr;
+  auto materialise = [&]() -> const uint32_t * {
+    if (psel && !rc) {
+      PRT_PROF("select_copy_u32", s);
+      select_copy_u32_kernel<<<g, 256, 0, s>>>(pa, pb, psel, n, perm);
+      pa = pb = perm;
+      psel = nullptr;
+    }
+    return pa;
+  };
   for (int p = 0; p < H && !rc; p++) {
     // segment size fanout^(H-p), saturated at n
     int64_t seg = 1;
@@ -898,10 +1001,9 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
     int seg_bits = 0;
     while ((1ll << seg_bits) < nseg) seg_bits++;
     const int use_y = p & 1;
-    const uint32_t *cur = have_perm ? perm : nullptr;
     if (seg <= kTdLocal) {
       // this and every later level have short runs: all of them sorted in
-      // shared memory by one launch, into tmp
+      // shared memory by one launch
       TdLocalLevels lv;
       lv.count = 0;
       for (int q = p; q < H && lv.count < kTdMaxLocal; q++) {
@@ -914,31 +1016,39 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
         lv.use_y[lv.count] = q & 1;
         lv.count++;
       }
+      uint32_t *out = (pa == tmp || pb == tmp) ? perm : tmp;
       rc = dispatch_coord(coord_type, [&](auto tag) {
         using T = decltype(tag);
-        return td_local_levels<T>(d_boxes, cur, n, lv, tmp, s);
+        return td_local_levels<T>(d_boxes, pa, pb, psel, n, lv, out, s);
       });
-      std::swap(perm, tmp);
+      pa = pb = out;
+      psel = nullptr;
       p += lv.count - 1;  // the loop's p++ moves past the last local level
     } else if (seg % kSortRunTile == 0 || seg == n) {
       // runs of whole sort tiles (or one run): every run sorted on its own by
-      // the coordinate alone, 4 (32-bit) or 8 (64-bit) passes
+      // the coordinate alone, 4 (32-bit) or 8 (64-bit) passes; the key kernel
+      // counts the digit histograms
       rc = dispatch_coord(coord_type, [&](auto tag) {
         using T = decltype(tag);
         using K = typename std::conditional<sizeof(T) == 8, uint64_t, uint32_t>::type;
         K *kk0 = reinterpret_cast<K *>(k0), *kk1 = reinterpret_cast<K *>(k1);
+        const int64_t tiles = (n + kSortRunTile - 1) / kSortRunTile;
+        const int64_t tpr = seg == n ? tiles : seg / kSortRunTile;
+        PRT_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (size_t)((tiles + tpr - 1) / tpr) * sizeof(K) * 256, s));
         {
           PRT_PROF("td_key", s);
-          td_keyrun_kernel<T, K><<<g, 256, 0, s>>>(reinterpret_cast<const Box<T> *>(d_boxes), cur, n, use_y, kk0, v0);
+          td_keyrun_kernel<T, K><<<(unsigned)tiles, 256, 0, s>>>(reinterpret_cast<const Box<T> *>(d_boxes), pa, pb,
+                                                                 psel, n, use_y, tpr, kk0, v0, hist);
         }
-        int r2 = seg == n ? radix_sort_pairs<K>(kk0, v0, kk1, v1, n, 8 * (int)sizeof(K), sel, err, s)
-                          : radix_sort_runs<K>(kk0, v0, kk1, v1, n, seg, sel, err, s);
-        if (r2) return r2;
-        PRT_PROF("select_copy_u32", s);
-        select_copy_u32_kernel<<<g, 256, 0, s>>>(v0, v1, sel, n, perm);
-        return PRT_OK;
+        PRT_CUDA(cudaGetLastError());
+        return seg == n ? radix_sort_pairs<K>(kk0, v0, kk1, v1, n, 8 * (int)sizeof(K), sel, err, s, hist)
+                        : radix_sort_runs<K>(kk0, v0, kk1, v1, n, seg, sel, err, s, hist);
       });
+      pa = v0;
+      pb = v1;
+      psel = sel;
     } else if (!wide) {
+      const uint32_t *cur = materialise();
       rc = dispatch_coord(coord_type, [&](auto tag) {
         using T = decltype(tag);
         if constexpr (sizeof(T) == 4) {
@@ -951,11 +1061,11 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
         return PRT_OK;
       });
       if (!rc) rc = radix_sort_pairs<uint64_t>(k0, v0, k1, v1, n, 32 + seg_bits, sel, err, s);
-      if (!rc) {
-        PRT_PROF("select_copy_u32", s);
-        select_copy_u32_kernel<<<g, 256, 0, s>>>(v0, v1, sel, n, perm);
-      }
+      pa = v0;
+      pb = v1;
+      psel = sel;
     } else {
+      const uint32_t *cur = materialise();
       rc = dispatch_coord(coord_type, [&](auto tag) {
         using T = decltype(tag);
         if constexpr (sizeof(T) == 8) {
@@ -995,12 +1105,13 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
         }
         cudaMemcpyAsync(perm, v0, 4 * n, cudaMemcpyDeviceToDevice, s);
       }
+      pa = pb = perm;
+      psel = nullptr;
     }
-    have_perm = true;
   }
   if (!rc) rc = dispatch_coord(coord_type, [&](auto tag) {
     using T = decltype(tag);
-    return pack_tree<T>(t, d_boxes, d_ids, perm, perm, nullptr, s);
+    return pack_tree<T>(t, d_boxes, d_ids, pa, pb, psel, s);
   });
   rc = finish(err, s, rc);
   dfree(scr, s);

@@ -202,10 +202,11 @@ int radix_sort_pairs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1,
 // The same sort applied to every run of run_len consecutive pairs
 // independently (all bits of the keys; the last run may be shorter): each run
 // ends sorted in place of itself.  run_len must be a multiple of the sort's
-// 4096-key tile.
+// 4096-key tile.  d_hist, when given, holds every run's digit histograms
+// (runs x passes x 256).
 template <typename KeyT>
 int radix_sort_runs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1, int64_t n, int64_t run_len,
-                    int *d_sel, unsigned *d_err, cudaStream_t s);
+                    int *d_sel, unsigned *d_err, cudaStream_t s, const uint32_t *d_hist = nullptr);
 constexpr int64_t kSortRunTile = 4096;
 
 // Exclusive prefix sum of n values into d_out (int64); *d_total (device,

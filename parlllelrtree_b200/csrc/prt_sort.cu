@@ -369,7 +369,7 @@ __global__ void run_plan_final_kernel(const int *__restrict__ trivial, int passe
 
 template <typename KeyT>
 int radix_sort_runs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1, int64_t n, int64_t run_len,
-                    int *d_sel, unsigned *d_err, cudaStream_t s) {
+                    int *d_sel, unsigned *d_err, cudaStream_t s, const uint32_t *d_hist) {
   PRT_CHECK(n >= 0 && n < (int64_t)kCountMask, PRT_ERR_INVALID, "radix sort: n=%lld out of range",
             (long long)n);
   PRT_CHECK(run_len >= kTile && run_len % kTile == 0, PRT_ERR_INVALID,
@@ -402,14 +402,15 @@ int radix_sort_runs(KeyT *keys0, uint32_t *vals0, KeyT *keys1, uint32_t *vals1, 
   cudaError_t e = cudaMemsetAsync(scratch, 0, total, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(trivial, 0xFF, sizeof(int) * passes, s);  // nonzero = trivial
   if (e == cudaSuccess) {
-    {
+    if (!d_hist) {
       PRT_PROF("run_hist", s);
       run_hist_kernel<KeyT><<<(unsigned)tiles, 256, sizeof(uint32_t) * passes * kRadix, s>>>(keys0, n, passes, tpr,
                                                                                             hist);
     }
     {
       PRT_PROF("plan", s);
-      run_plan_kernel<<<(unsigned)runs, kRadix, 0, s>>>(hist, n, run_len, runs, passes, goff, trivial);
+      run_plan_kernel<<<(unsigned)runs, kRadix, 0, s>>>(d_hist ? d_hist : hist, n, run_len, runs, passes, goff,
+                                                        trivial);
       run_plan_final_kernel<<<1, 1, 0, s>>>(trivial, passes, plan, d_sel);
     }
     size_t smem = sizeof(PassSmem<KeyT>);
@@ -506,9 +507,9 @@ std::atomic<int> g_wait_blind{0};
 WaitLimit wait_limit() { return WaitLimit{g_wait_polls.load(), g_wait_blind.load()}; }
 
 template int radix_sort_runs<uint32_t>(uint32_t *, uint32_t *, uint32_t *, uint32_t *, int64_t, int64_t, int *,
-                                       unsigned *, cudaStream_t);
+                                       unsigned *, cudaStream_t, const uint32_t *);
 template int radix_sort_runs<uint64_t>(uint64_t *, uint32_t *, uint64_t *, uint32_t *, int64_t, int64_t, int *,
-                                       unsigned *, cudaStream_t);
+                                       unsigned *, cudaStream_t, const uint32_t *);
 template int radix_sort_pairs<uint32_t>(uint32_t *, uint32_t *, uint32_t *, uint32_t *, int64_t, int, int *,
                                         unsigned *, cudaStream_t, const uint32_t *);
 template int radix_sort_pairs<uint64_t>(uint64_t *, uint32_t *, uint64_t *, uint32_t *, int64_t, int, int *,
