@@ -146,20 +146,22 @@ __device__ void pieces(const Poly &A, const Poly &B, double w, double *grad, int
 // summed across neighbouring lanes before the atomics.  Edges with more than
 // kBwdMaxT crossings take the global-memory path (next_crossing).
 constexpr int kBwdMaxV = 128;
+constexpr int kBwdSmallV = 64;
 constexpr int kBwdMaxT = 16;
 constexpr int kBwdWarps = 4;
 constexpr int kSlabs = 32;
 constexpr unsigned kFullMask = 0xffffffffu;
 
-struct BwdPoly {  // one polygon in shared memory
-  float4 bb[kBwdMaxV];                    // edge k's box (x_lo, y_lo, x_hi, y_hi), rounded outwards
-  double x[kBwdMaxV], y[kBwdMaxV];
-  uint32_t slab[kBwdMaxV / 32][kSlabs];   // y slabs: word c of slab s, bit k = edge 32 c + k reaches slab s
-  uint32_t xslab[kBwdMaxV / 32][kSlabs];  // the same for x slabs
+template <int V>
+struct BwdPoly {  // one polygon in shared memory (up to V vertices)
+  float4 bb[V];                    // edge k's box (x_lo, y_lo, x_hi, y_hi), rounded outwards
+  double x[V], y[V];
+  uint32_t slab[V / 32][kSlabs];   // y slabs: word c of slab s, bit k = edge 32 c + k reaches slab s
+  uint32_t xslab[V / 32][kSlabs];  // the same for x slabs
   int16_t ringv[33];                      // first vertex of ring r; ringv[rings] = the vertex count
-  int8_t sgn[kBwdMaxV];                   // orientation sign of edge k (0: ring of < 2 vertices)
-  uint8_t nxt[kBwdMaxV];                  // end vertex of edge k
-  uint8_t rst[kBwdMaxV];                  // first vertex of edge k's ring
+  int8_t sgn[V];                   // orientation sign of edge k (0: ring of < 2 vertices)
+  uint8_t nxt[V];                  // end vertex of edge k
+  uint8_t rst[V];                  // first vertex of edge k's ring
 };
 
 // coordinate -> slab: monotone non-decreasing (round-to-nearest float steps
@@ -181,10 +183,11 @@ __device__ inline SlabGrid slab_grid(float lo, float hi) {
 // [rb0, rb1) of LB) with their ring links, orientation signs and edge boxes;
 // the loads of the two are issued together.  nv[p] is polygon p's vertex
 // count, vb[p] its first vertex, ext[p] the float extent of its edge boxes.
-// Returns false (nothing staged) when a polygon has more than kBwdMaxV
+// Returns false (nothing staged) when a polygon has more than V
 // vertices or more than 31 rings.
+template <int V>
 __device__ inline bool bwd_load_pair(const LayerDev &LA, int64_t ra0, int64_t ra1, const LayerDev &LB, int64_t rb0,
-                                     int64_t rb1, BwdPoly *M, int *nv, int64_t *vb, float4 *ext) {
+                                     int64_t rb1, BwdPoly<V> *M, int *nv, int64_t *vb, float4 *ext) {
   const int lane = threadIdx.x & 31;
   const int nr[2] = {(int)(ra1 - ra0), (int)(rb1 - rb0)};
   if (nr[0] > 31 || nr[1] > 31) return false;
@@ -199,21 +202,21 @@ __device__ inline bool bwd_load_pair(const LayerDev &LA, int64_t ra0, int64_t ra
     vb[p] = __shfl_sync(kFullMask, rv[p], 0);
     nv[p] = (int)(__shfl_sync(kFullMask, rv[p], nr[p]) - vb[p]);
   }
-  if (nv[0] > kBwdMaxV || nv[1] > kBwdMaxV) return false;
+  if (nv[0] > V || nv[1] > V) return false;
 #pragma unroll
   for (int p = 0; p < 2; p++)
     if (lane <= nr[p]) M[p].ringv[lane] = (int16_t)(rv[p] - vb[p]);
   __syncwarp();
   const float inf = __int_as_float(0x7f800000);
   float4 e[2] = {make_float4(inf, inf, -inf, -inf), make_float4(inf, inf, -inf, -inf)};
-  double term[2][kBwdMaxV / 32];  // shoelace terms of this lane's vertices
-  int rix[2][kBwdMaxV / 32];      // and their rings
+  double term[2][V / 32];  // shoelace terms of this lane's vertices
+  int rix[2][V / 32];      // and their rings
 #pragma unroll
-  for (int t = 0; t < kBwdMaxV / 32; t++) {
+  for (int t = 0; t < V / 32; t++) {
 #pragma unroll
     for (int p = 0; p < 2; p++) {
       const LayerDev &L = p ? LB : LA;
-      BwdPoly &Q = M[p];
+      BwdPoly<V> &Q = M[p];
       const int i = 32 * t + lane;
       term[p][t] = 0.0;
       rix[p][t] = -1;
@@ -242,13 +245,13 @@ __device__ inline bool bwd_load_pair(const LayerDev &LA, int64_t ra0, int64_t ra
     for (int r = 0; r < nr[p]; r++) {
       double sa = 0.0;
 #pragma unroll
-      for (int t = 0; t < kBwdMaxV / 32; t++) sa += rix[p][t] == r ? term[p][t] : 0.0;
+      for (int t = 0; t < V / 32; t++) sa += rix[p][t] == r ? term[p][t] : 0.0;
       for (int o = 16; o; o >>= 1) sa += __shfl_xor_sync(kFullMask, sa, o);
       const bool hole = __shfl_sync(kFullMask, hl[p], r) != 0;
       const int n = M[p].ringv[r + 1] - M[p].ringv[r];
       const int8_t sg = n < 2 ? 0 : (int8_t)((sa >= 0.0 ? 1 : -1) * (hole ? -1 : 1));
 #pragma unroll
-      for (int t = 0; t < kBwdMaxV / 32; t++)
+      for (int t = 0; t < V / 32; t++)
         if (rix[p][t] == r) M[p].sgn[32 * t + lane] = sg;
     }
     for (int o = 16; o; o >>= 1) {
@@ -278,7 +281,8 @@ __device__ inline uint32_t bit_transpose(uint32_t x) {
 
 // y and x slab masks of both staged polygons (four independent transposes
 // per word).
-__device__ inline void bwd_slabs(BwdPoly *M, const int *nv, const SlabGrid &gy, const SlabGrid &gx) {
+template <int V>
+__device__ inline void bwd_slabs(BwdPoly<V> *M, const int *nv, const SlabGrid &gy, const SlabGrid &gx) {
   const int lane = threadIdx.x & 31;
   const int nw = ((nv[0] > nv[1] ? nv[0] : nv[1]) + 31) / 32;
   for (int c = 0; c < nw; c++) {
@@ -321,7 +325,8 @@ __device__ __noinline__ void bwd_edge_global(const Poly &Qg, double px, double p
 
 // Even-odd test of (mx, my) against staged polygon Q through the slab of
 // my: inside_evenodd's expression over the edges that can straddle my.
-__device__ inline bool bwd_inside(const BwdPoly &Q, int nwq, const float4 &qe, const SlabGrid &g, double mx,
+template <int V>
+__device__ inline bool bwd_inside(const BwdPoly<V> &Q, int nwq, const float4 &qe, const SlabGrid &g, double mx,
                                   double my) {
   const float fy = __double2float_rn(my);
   if (fy < qe.y || fy > qe.w) return false;  // no edge of Q straddles my
@@ -346,7 +351,8 @@ __device__ inline bool bwd_inside(const BwdPoly &Q, int nwq, const float4 &qe, c
 
 // Candidate edges of Q (mask word c) for an edge whose box covers y slabs
 // [s0, s1] and x slabs [x0, x1].
-__device__ inline uint32_t bwd_cands(const BwdPoly &Q, int c, int s0, int s1, int x0, int x1) {
+template <int V>
+__device__ inline uint32_t bwd_cands(const BwdPoly<V> &Q, int c, int s0, int s1, int x0, int x1) {
   uint32_t ybits = 0, xbits = 0;
   for (int s = s0; s <= s1; s++) ybits |= Q.slab[c][s];
   for (int s = x0; s <= x1; s++) xbits |= Q.xslab[c][s];
@@ -356,7 +362,8 @@ __device__ inline uint32_t bwd_cands(const BwdPoly &Q, int c, int s0, int s1, in
 // One edge p -> p + r against staged polygon Q by the definition: every
 // crossing by next_crossing's test (kBwdMaxT at most, else the global-memory
 // path), sorted and deduplicated, and every interval by its midpoint.
-__device__ __noinline__ void bwd_edge_exact(const BwdPoly &Q, int nwq, const float4 &qe, const SlabGrid &g,
+template <int V>
+__device__ __noinline__ void bwd_edge_exact(const BwdPoly<V> &Q, int nwq, const float4 &qe, const SlabGrid &g,
                                             const SlabGrid &gx, const float4 &pb, double px, double py, double rx,
                                             double ry, const Poly &Qg, double *it_out, double *i1_out) {
   double ts[kBwdMaxT];
@@ -448,8 +455,8 @@ struct AreaSum {
 // Returns false in area mode as soon as any crossing of the pair is unclean
 // (the caller then clips the pair with GPC); in gradient mode it always runs
 // to the end, by the definition from the first unclean crossing on.
-template <bool kArea>
-__device__ inline bool pair_boundary(const BwdPoly *M, const float4 *ext, int na, int nb, const SlabGrid &g,
+template <bool kArea, int V>
+__device__ inline bool pair_boundary(const BwdPoly<V> *M, const float4 *ext, int na, int nb, const SlabGrid &g,
                                      const SlabGrid &gx, double w, double *ga, double *gb, int64_t va, int64_t vb,
                                      const Poly &Ag, const Poly &Bg, double ox, double oy, AreaSum *acc) {
   const int lane = threadIdx.x & 31;
@@ -461,7 +468,7 @@ __device__ inline bool pair_boundary(const BwdPoly *M, const float4 *ext, int na
     const int e = e0 + lane;
     const int side = e < na ? 0 : 1;
     const int i = side ? e - na : e;
-    const BwdPoly &P = M[side], &Q = M[1 - side];
+    const BwdPoly<V> &P = M[side], &Q = M[1 - side];
     const int nwq = ((side ? na : nb) + 31) >> 5;
     const bool valid = e < na + nb && P.sgn[i] != 0;
     const int j = valid ? P.nxt[i] : 0;
@@ -548,7 +555,7 @@ __device__ inline bool pair_boundary(const BwdPoly *M, const float4 *ext, int na
         const int L = __ffs(q) - 1;
         const double mxl = __shfl_sync(kFullMask, mx0, L), myl = __shfl_sync(kFullMask, my0, L);
         const int sl = e0 + L < na ? 0 : 1;
-        const BwdPoly &QL = M[1 - sl];
+        const BwdPoly<V> &QL = M[1 - sl];
         const int nql = sl ? na : nb;
         bool in = false;
         for (int k = lane; k < nql; k += 32) {
@@ -634,33 +641,56 @@ __device__ inline bool pair_boundary(const BwdPoly *M, const float4 *ext, int na
   return true;
 }
 
-// Pairs with a polygon above kBwdMaxV vertices: the global-memory path.
+// Pairs with a polygon above V vertices: the global-memory path.
 __device__ __noinline__ void bwd_pair_global(const Poly &A, const Poly &B, double w, double *ga, double *gb) {
   const int lane = threadIdx.x & 31;
   pieces(A, B, w, ga, lane);
   pieces(B, A, w, gb, lane);
 }
 
-// 4 blocks of 4 warps per SM: 120 registers, no spills (5 blocks would cap
-// the kernel at 96 registers and spill)
+// Pair lists of the two-stage launches: the first stage (V = kBwdSmallV)
+// takes every pair and lists those with a polygon above V vertices (or 31
+// rings) in `defer`; the second stage (V = kBwdMaxV) takes only the listed
+// pairs (`sel`, *sel_count of them).
+struct PairList {
+  const int32_t *sel;                   // items of this launch (nullptr: pairs 0 .. n-1)
+  const unsigned long long *sel_count;  // how many (device)
+  int32_t *defer;                       // pairs this stage cannot stage (nullptr: none deferred)
+  unsigned long long *defer_count;
+};
+
+__device__ __forceinline__ int64_t list_items(const PairList &L, int64_t n) {
+  return L.sel ? (int64_t)min((unsigned long long)n, *L.sel_count) : n;
+}
+
+// 4 blocks of 4 warps per SM (120 registers, no spills; measured at 1M
+// pairs of 16-64-vertex stars, 5 blocks of the V = 64 kernel spill and run
+// 10% slower).
+template <int V>
 __global__ void __launch_bounds__(32 * kBwdWarps, 4) area_bwd_kernel(
     const int32_t *__restrict__ pa, const int32_t *__restrict__ pb, int64_t n, LayerDev base, LayerDev over,
-    const double *__restrict__ upstream, double *grad_base, double *grad_over) {
-  __shared__ BwdPoly sm[kBwdWarps][2];
-  BwdPoly *M = sm[threadIdx.x >> 5];
+    const double *__restrict__ upstream, double *grad_base, double *grad_over, PairList PL) {
+  __shared__ BwdPoly<V> sm[kBwdWarps][2];
+  BwdPoly<V> *M = sm[threadIdx.x >> 5];
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t items = list_items(PL, n);
   // a pair's ids are read one pair ahead and its ring ranges half a pair
   // ahead, so the staging of a pair waits only for its ring starts and
   // vertices
-  auto ids = [&](int64_t k, int64_t *a, int64_t *b) {
+  auto ids = [&](int64_t k, int64_t *i, int64_t *a, int64_t *b) {
+    *i = -1;
     *a = -1;
     *b = -1;
-    if (k < n) {
-      const int64_t x = pa[k], y = pb[k];
-      if (x >= 0 && x < base.n_poly && y >= 0 && y < over.n_poly) {
-        *a = x;
-        *b = y;
+    if (k < items) {
+      const int64_t j = PL.sel ? PL.sel[k] : k;
+      if (j >= 0 && j < n) {
+        const int64_t x = pa[j], y = pb[j];
+        if (x >= 0 && x < base.n_poly && y >= 0 && y < over.n_poly) {
+          *i = j;
+          *a = x;
+          *b = y;
+        }
       }
     }
   };
@@ -673,15 +703,14 @@ __global__ void __launch_bounds__(32 * kBwdWarps, 4) area_bwd_kernel(
       r[3] = over.poly_ring[b + 1];
     }
   };
-  int64_t a, b, rr[4];
-  ids(warp, &a, &b);
+  int64_t i, a, b, rr[4];
+  ids(warp, &i, &a, &b);
   rings(a, b, rr);
-  for (int64_t i = warp; i < n; i += nw) {
-    int64_t an, bn, rn[4];
-    ids(i + nw, &an, &bn);
+  for (int64_t k = warp; k < items; k += nw) {
+    int64_t in, an, bn, rn[4];
+    ids(k + nw, &in, &an, &bn);
     bool fetched = false;
     if (a >= 0) {
-      const double w = upstream ? upstream[i] : 1.0;
       int nv[2];
       int64_t vb[2];
       float4 ext[2];
@@ -689,6 +718,7 @@ __global__ void __launch_bounds__(32 * kBwdWarps, 4) area_bwd_kernel(
       rings(an, bn, rn);
       fetched = true;
       if (staged) {
+        const double w = upstream ? upstream[i] : 1.0;
         // boxes apart: no crossings and no midpoint inside the other polygon
         const float x0 = fmaxf(ext[0].x, ext[1].x), x1 = fminf(ext[0].z, ext[1].z);
         const float y0 = fmaxf(ext[0].y, ext[1].y), y1 = fminf(ext[0].w, ext[1].w);
@@ -700,16 +730,20 @@ __global__ void __launch_bounds__(32 * kBwdWarps, 4) area_bwd_kernel(
           pair_boundary<false>(M, ext, nv[0], nv[1], gy, gx, w, grad_base, grad_over, vb[0], vb[1], A, B, 0.0,
                                0.0, nullptr);
         }
+      } else if (PL.defer) {
+        if ((threadIdx.x & 31) == 0) PL.defer[atomicAdd(PL.defer_count, 1ull)] = (int32_t)i;
       } else {
+        const double w = upstream ? upstream[i] : 1.0;
         Poly A{base.ring_vert, base.ring_hole, base.xy, rr[0], rr[1]};
         Poly B{over.ring_vert, over.ring_hole, over.xy, rr[2], rr[3]};
         bwd_pair_global(A, B, w, grad_base, grad_over);
       }
     }
     if (!fetched) rings(an, bn, rn);
+    i = in;
     a = an;
     b = bn;
-    for (int k = 0; k < 4; k++) rr[k] = rn[k];
+    for (int q = 0; q < 4; q++) rr[q] = rn[q];
     __syncwarp();
   }
 }
@@ -717,7 +751,7 @@ __global__ void __launch_bounds__(32 * kBwdWarps, 4) area_bwd_kernel(
 // Forward: one warp per pair, staged as in the backward.  A pair gets its
 // area from pair_boundary's area mode when every crossing is clean and the
 // crossing error bound stays below kFwdTol of the area; every other pair
-// (polygons above kBwdMaxV vertices or 31 rings, unclean crossings, slivers
+// (polygons above V vertices or 31 rings, unclean crossings, slivers
 // whose area the bound does not pin to kFwdTol, ids out of range) is listed in
 // fb[] for the GPC clip.  GPC intersects the same edges, so for a clean pair
 // the two areas differ only by where each side rounds the crossing vertices:
@@ -733,18 +767,24 @@ constexpr double kFwdTol = 1e-10;
 // Pairs the last forward call listed for the GPC clip (prt_area_fwd_fallbacks).
 std::atomic<int64_t> g_fwd_fallbacks{0};
 
-__global__ void __launch_bounds__(32 * kBwdWarps, 4) area_fwd_kernel(
+// V = 64: 5 blocks of 4 warps per SM (96 registers: a few spills, 10% faster
+// than 4 blocks at 1M pairs of 16-64-vertex stars).
+template <int V>
+__global__ void __launch_bounds__(32 * kBwdWarps, V <= kBwdSmallV ? 5 : 4) area_fwd_kernel(
     const int32_t *__restrict__ pa, const int32_t *__restrict__ pb, int64_t n, LayerDev base, LayerDev over,
-    double *__restrict__ area, int32_t *__restrict__ fb, unsigned long long *__restrict__ fb_count) {
-  __shared__ BwdPoly sm[kBwdWarps][2];
-  BwdPoly *M = sm[threadIdx.x >> 5];
+    double *__restrict__ area, int32_t *__restrict__ fb, unsigned long long *__restrict__ fb_count, PairList PL) {
+  __shared__ BwdPoly<V> sm[kBwdWarps][2];
+  BwdPoly<V> *M = sm[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t items = list_items(PL, n);
   auto fallback = [&](int64_t i) {
     if (lane == 0) fb[atomicAdd(fb_count, 1ull)] = (int32_t)i;
   };
-  for (int64_t i = warp; i < n; i += nw) {
+  for (int64_t k = warp; k < items; k += nw) {
+    const int64_t i = PL.sel ? PL.sel[k] : k;
+    if (i < 0 || i >= n) continue;
     const int64_t a = pa[i], b = pb[i];
     if (a < 0 || a >= base.n_poly || b < 0 || b >= over.n_poly) {
       fallback(i);  // the clip reports the bad id
@@ -757,7 +797,11 @@ __global__ void __launch_bounds__(32 * kBwdWarps, 4) area_fwd_kernel(
     float4 ext[2];
     const bool staged = bwd_load_pair(base, ra0, ra1, over, rb0, rb1, M, nv, vb, ext);
     if (!staged) {
-      fallback(i);
+      if (PL.defer) {
+        if (lane == 0) PL.defer[atomicAdd(PL.defer_count, 1ull)] = (int32_t)i;
+      } else {
+        fallback(i);
+      }
       __syncwarp();
       continue;
     }
@@ -838,17 +882,24 @@ int prt_area_fwd(const int32_t *d_pair_a, const int32_t *d_pair_b, int64_t n_pai
   PRT_CHECK(n_pairs >= 0 && n_pairs < (1ll << 31), PRT_ERR_INVALID, "n_pairs=%lld", (long long)n_pairs);
   if (n_pairs == 0) return PRT_OK;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  // boundary integral for the clean pairs, the list of the others
+  // boundary integral for the clean pairs, the list of the others; pairs
+  // with a polygon above kBwdSmallV vertices go through the second stage
   unsigned char *scr = nullptr;
-  int rc = dmalloc(reinterpret_cast<void **>(&scr), 64 + 4 * (size_t)n_pairs, s);
+  int rc = dmalloc(reinterpret_cast<void **>(&scr), 64 + 8 * (size_t)n_pairs, s);
   if (rc) return rc;
   unsigned long long *cnt = reinterpret_cast<unsigned long long *>(scr);
+  unsigned long long *dcnt = cnt + 1;
   int32_t *fb = reinterpret_cast<int32_t *>(scr + 64);
-  cudaError_t e = cudaMemsetAsync(cnt, 0, 8, s);
+  int32_t *defer = fb + n_pairs;
+  cudaError_t e = cudaMemsetAsync(cnt, 0, 16, s);
   if (e == cudaSuccess) {
     PRT_PROF("area_fwd", s);
-    area_fwd_kernel<<<area_blocks(n_pairs, (const void *)area_fwd_kernel), 32 * kBwdWarps, 0, s>>>(
-      d_pair_a, d_pair_b, n_pairs, layer_dev(base), layer_dev(overlay), d_area, fb, cnt);
+    area_fwd_kernel<kBwdSmallV><<<area_blocks(n_pairs, (const void *)area_fwd_kernel<kBwdSmallV>), 32 * kBwdWarps,
+                                  0, s>>>(d_pair_a, d_pair_b, n_pairs, layer_dev(base), layer_dev(overlay), d_area, fb,
+                                          cnt, PairList{nullptr, nullptr, defer, dcnt});
+    area_fwd_kernel<kBwdMaxV><<<area_blocks(n_pairs, (const void *)area_fwd_kernel<kBwdMaxV>), 32 * kBwdWarps, 0,
+                                s>>>(d_pair_a, d_pair_b, n_pairs, layer_dev(base), layer_dev(overlay), d_area, fb,
+                                     cnt, PairList{defer, dcnt, nullptr, nullptr});
     e = cudaGetLastError();
   }
   unsigned long long m = 0;
@@ -906,13 +957,27 @@ int prt_area_bwd(const int32_t *d_pair_a, const int32_t *d_pair_b, int64_t n_pai
             PRT_ERR_INVALID, "NULL argument");
   if (n_pairs == 0) return PRT_OK;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  {
+  // pairs with a polygon above kBwdSmallV vertices: listed by the first
+  // stage, taken by the second
+  unsigned char *scr = nullptr;
+  int rc = dmalloc(reinterpret_cast<void **>(&scr), 64 + 4 * (size_t)n_pairs, s);
+  if (rc) return rc;
+  unsigned long long *dcnt = reinterpret_cast<unsigned long long *>(scr);
+  int32_t *defer = reinterpret_cast<int32_t *>(scr + 64);
+  cudaError_t e = cudaMemsetAsync(dcnt, 0, 8, s);
+  if (e == cudaSuccess) {
     PRT_PROF("area_bwd", s);
-    const int blocks = area_blocks(n_pairs, (const void *)area_bwd_kernel);
-    area_bwd_kernel<<<blocks, 32 * kBwdWarps, 0, s>>>(d_pair_a, d_pair_b, n_pairs, layer_dev(base),
-                                                      layer_dev(overlay), d_upstream, d_grad_base, d_grad_overlay);
+    area_bwd_kernel<kBwdSmallV><<<area_blocks(n_pairs, (const void *)area_bwd_kernel<kBwdSmallV>), 32 * kBwdWarps,
+                                  0, s>>>(d_pair_a, d_pair_b, n_pairs, layer_dev(base), layer_dev(overlay),
+                                          d_upstream, d_grad_base, d_grad_overlay,
+                                          PairList{nullptr, nullptr, defer, dcnt});
+    area_bwd_kernel<kBwdMaxV><<<area_blocks(n_pairs, (const void *)area_bwd_kernel<kBwdMaxV>), 32 * kBwdWarps, 0,
+                                s>>>(d_pair_a, d_pair_b, n_pairs, layer_dev(base), layer_dev(overlay), d_upstream,
+                                     d_grad_base, d_grad_overlay, PairList{defer, dcnt, nullptr, nullptr});
+    e = cudaGetLastError();
   }
-  PRT_CUDA(cudaGetLastError());
+  dfree(scr, s);
+  if (e != cudaSuccess) return cuda_status(e, "area backward");
   return PRT_OK;
 }
 

@@ -25,10 +25,11 @@ def overlapping_pairs(n, seed, nv_lo=16, nv_hi=64, hole_frac=0.0):
     return A, B
 
 
-@pytest.mark.parametrize("hole_frac,nv", [(0.0, (16, 64)), (0.5, (16, 64)), (0.3, (100, 200))])
+@pytest.mark.parametrize("hole_frac,nv", [(0.0, (16, 64)), (0.5, (16, 64)), (0.0, (40, 100)), (0.3, (100, 200))])
 def test_forward_and_adjoint_match_oracle(cuda, hole_frac, nv):
-    """Pairs of up to 128 vertices per polygon take the slab-indexed adjoint,
-    larger ones the brute-force one; both must give the oracle's gradient."""
+    """Pairs of up to 64 vertices per polygon take the first slab-indexed
+    stage, up to 128 the second, larger ones the brute-force adjoint; all
+    must give the oracle's area and gradient."""
     import parlllelrtree_b200 as prt
 
     n = 2000 if nv[1] <= 64 else 300
