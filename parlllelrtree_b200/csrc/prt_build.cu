@@ -553,13 +553,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) td_local_sort_ker
           d = (int)(v & ((1u << width) - 1u));
           it[j] = x;
         }
+        // eight ballots whatever the width: a live item's bits above it are 0
         uint32_t peers = __ballot_sync(0xffffffffu, ok);
 #pragma unroll
         for (int bit = 0; bit < 8; bit++) {
-          if (bit < width) {
-            const uint32_t bm = __ballot_sync(0xffffffffu, (d >> bit) & 1);
-            peers &= ((d >> bit) & 1) ? bm : ~bm;
-          }
+          const uint32_t bm = __ballot_sync(0xffffffffu, (d >> bit) & 1);
+          peers &= ((d >> bit) & 1) ? bm : ~bm;
         }
         if (!ok) peers = 1u << lane;
         const int leader = __ffs(peers) - 1;
