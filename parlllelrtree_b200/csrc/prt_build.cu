@@ -336,19 +336,22 @@ __device__ __forceinline__ const uint32_t *cur_perm(const uint32_t *perm_a, cons
 // histograms hist[(run * passes + p) * 256 + digit], so the sort does not
 // read the keys again to count them.  The order is read and the values
 // written at the same positions by the same thread: vals may be the buffer
-// the order is read from.
+// the order is read from.  Record r's (x1, y1) is at c[stride * r] (the boxes,
+// stride 4, or the compact copy, stride 2); with the identity order the
+// kernel can write that compact copy (xy_out), so later levels gather from
+// an array a quarter (float) of the boxes' size, which stays in L2.
 template <typename T, typename K>
-__global__ void __launch_bounds__(256) td_keyrun_kernel(const Box<T> *__restrict__ b, const uint32_t *perm_a,
+__global__ void __launch_bounds__(256) td_keyrun_kernel(const T *__restrict__ cxy, int stride, const uint32_t *perm_a,
                                                         const uint32_t *perm_b, const int *sel, int64_t n, int use_y,
                                                         int64_t tiles_per_run, K *__restrict__ keys, uint32_t *vals,
-                                                        uint32_t *__restrict__ hist) {
+                                                        uint32_t *__restrict__ hist, T *__restrict__ xy_out) {
   constexpr int kPasses = (int)sizeof(K);
   constexpr int kPer = (int)(kSortRunTile / 256);
   __shared__ uint32_t sh[kPasses * 256];
   for (int i = threadIdx.x; i < kPasses * 256; i += 256) sh[i] = 0;
   __syncthreads();
   const uint32_t *perm = cur_perm(perm_a, perm_b, sel);
-  const T *c = reinterpret_cast<const T *>(b) + (use_y ? 1 : 0);
+  const T *c = cxy + (use_y ? 1 : 0);
   const int64_t base = (int64_t)blockIdx.x * kSortRunTile + threadIdx.x;
   // all loads of the order first, then all coordinate loads, then the stores
   uint32_t r[kPer];
@@ -360,7 +363,17 @@ __global__ void __launch_bounds__(256) td_keyrun_kernel(const Box<T> *__restrict
   }
   K k[kPer];
 #pragma unroll
-  for (int j = 0; j < kPer; j++) k[j] = base + 256 * j < n ? (K)ukey(__ldg(&c[4 * (int64_t)r[j]])) : K(0);
+  for (int j = 0; j < kPer; j++) k[j] = base + 256 * j < n ? (K)ukey(__ldg(&c[stride * (int64_t)r[j]])) : K(0);
+  if (xy_out) {  // identity order: record i's (x1, y1), read in order
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+      const int64_t i = base + 256 * j;
+      if (i < n) {
+        xy_out[2 * i] = cxy[stride * i];
+        xy_out[2 * i + 1] = cxy[stride * i + 1];
+      }
+    }
+  }
 #pragma unroll
   for (int j = 0; j < kPer; j++) {
     const int64_t i = base + 256 * j;
@@ -467,9 +480,9 @@ __device__ __forceinline__ int bit_length(uint64_t x) { return 64 - __clzll((lon
 // them, in 8-bit digits (the last one narrower).  Subtracting one constant
 // from every key keeps their order, so this is the order of a stable sort by
 // key within each run.
-template <typename T>
+template <typename T, int kStride>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) td_local_sort_kernel(
-    const Box<T> *__restrict__ b, const uint32_t *__restrict__ perm_a, const uint32_t *__restrict__ perm_b,
+    const T *__restrict__ c, const uint32_t *__restrict__ perm_a, const uint32_t *__restrict__ perm_b,
     const int *__restrict__ sel, int64_t n, TdLocalLevels lv, uint32_t *__restrict__ perm_out) {
   using K = typename std::conditional<sizeof(T) == 8, uint64_t, uint32_t>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -478,13 +491,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) td_local_sort_ker
   const int64_t chunk = (kTdLocal / lv.seg[0]) * lv.seg[0];  // whole runs of the first local level
   const int64_t base = blockIdx.x * chunk;
   const int m = (int)min(chunk, n - base);
-  const T *c = reinterpret_cast<const T *>(b);
   const uint32_t *perm_in = cur_perm(perm_a, perm_b, sel);
   for (int i = tid; i < m; i += 256) {
     uint32_t r = perm_in ? perm_in[base + i] : (uint32_t)(base + i);
     if ((int64_t)r >= n) r = 0;  // only after a timed-out sort (reported by the caller)
-    S.xy[i][0] = __ldg(&c[4 * (int64_t)r]);
-    S.xy[i][1] = __ldg(&c[4 * (int64_t)r + 1]);
+    S.xy[i][0] = __ldg(&c[kStride * (int64_t)r]);
+    S.xy[i][1] = __ldg(&c[kStride * (int64_t)r + 1]);
     S.item[0][i] = (uint32_t)i;
   }
   const uint32_t lt = lane_lt();
@@ -614,22 +626,25 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) td_local_sort_ker
 // Launches the short-run sort of the local levels lv (first run length at
 // most kTdLocal, each next one dividing it).
 template <typename T>
-int td_local_levels(const void *d_boxes, const uint32_t *perm_a, const uint32_t *perm_b, const int *sel, int64_t n,
-                    const TdLocalLevels &lv, uint32_t *perm_out, cudaStream_t s) {
+int td_local_levels(const T *cxy, int stride, const uint32_t *perm_a, const uint32_t *perm_b, const int *sel,
+                    int64_t n, const TdLocalLevels &lv, uint32_t *perm_out, cudaStream_t s) {
   const int64_t chunk = (kTdLocal / lv.seg[0]) * lv.seg[0];
   const size_t smem = sizeof(TdLocalSmem<T>);
   static bool attr_done[256] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 256 || !attr_done[dev]) {
-    PRT_CUDA(cudaFuncSetAttribute(td_local_sort_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PRT_CUDA(cudaFuncSetAttribute(td_local_sort_kernel<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PRT_CUDA(cudaFuncSetAttribute(td_local_sort_kernel<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (dev >= 0 && dev < 256) attr_done[dev] = true;
   }
   const int64_t blocks = (n + chunk - 1) / chunk;
   {
     PRT_PROF("td_local_sort", s);
-    td_local_sort_kernel<T><<<(unsigned)blocks, 256, smem, s>>>(reinterpret_cast<const Box<T> *>(d_boxes), perm_a,
-                                                                perm_b, sel, n, lv, perm_out);
+    if (stride == 2)
+      td_local_sort_kernel<T, 2><<<(unsigned)blocks, 256, smem, s>>>(cxy, perm_a, perm_b, sel, n, lv, perm_out);
+    else
+      td_local_sort_kernel<T, 4><<<(unsigned)blocks, 256, smem, s>>>(cxy, perm_a, perm_b, sel, n, lv, perm_out);
   }
   PRT_CUDA(cudaGetLastError());
   return PRT_OK;
@@ -954,7 +969,9 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
   unsigned char *scr = nullptr;
   // per-run digit histograms: at most one run per sort tile, 8 passes
   const size_t hist_words = (size_t)((n + kSortRunTile - 1) / kSortRunTile) * 8 * 256;
-  size_t need = 64 + 2 * 8 * n + 4 * 4 * n + 4 * hist_words + 64;
+  // and the compact (x1, y1) copy the first level writes
+  const size_t csize = (size_t)coord_size(coord_type);
+  size_t need = 64 + 2 * 8 * n + 4 * 4 * n + 4 * hist_words + 2 * csize * n + 64;
   rc = dmalloc(reinterpret_cast<void **>(&scr), need, s);
   if (rc) {
     prt_tree_free(t);
@@ -969,6 +986,11 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
   uint32_t *perm = v1 + n;  // current leaf order (when materialised)
   uint32_t *tmp = perm + n;  // scratch
   uint32_t *hist = tmp + n;
+  void *xyc = hist + hist_words;
+  // where the levels read record r's (x1, y1): d_boxes[4 r], or the compact
+  // copy at xyc[2 r] once a level has written it
+  const void *cxy = d_boxes;
+  int cstride = 4;
   cudaError_t e = cudaMemsetAsync(err, 0, 8, s);
   if (e != cudaSuccess) rc = cuda_status(e, "memset");
   const int g = grid_for(n, 256, 16);
@@ -1018,7 +1040,7 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
       uint32_t *out = (pa == tmp || pb == tmp) ? perm : tmp;
       rc = dispatch_coord(coord_type, [&](auto tag) {
         using T = decltype(tag);
-        return td_local_levels<T>(d_boxes, pa, pb, psel, n, lv, out, s);
+        return td_local_levels<T>(reinterpret_cast<const T *>(cxy), cstride, pa, pb, psel, n, lv, out, s);
       });
       pa = pb = out;
       psel = nullptr;
@@ -1034,10 +1056,16 @@ int prt_build_topdown(const void *d_boxes, int coord_type, const int32_t *d_ids,
         const int64_t tiles = (n + kSortRunTile - 1) / kSortRunTile;
         const int64_t tpr = seg == n ? tiles : seg / kSortRunTile;
         PRT_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (size_t)((tiles + tpr - 1) / tpr) * sizeof(K) * 256, s));
+        // the identity order reads the boxes in order: write the compact copy
+        T *xy_out = (pa == nullptr && cstride == 4) ? reinterpret_cast<T *>(xyc) : nullptr;
         {
           PRT_PROF("td_key", s);
-          td_keyrun_kernel<T, K><<<(unsigned)tiles, 256, 0, s>>>(reinterpret_cast<const Box<T> *>(d_boxes), pa, pb,
-                                                                 psel, n, use_y, tpr, kk0, v0, hist);
+          td_keyrun_kernel<T, K><<<(unsigned)tiles, 256, 0, s>>>(reinterpret_cast<const T *>(cxy), cstride, pa, pb,
+                                                                 psel, n, use_y, tpr, kk0, v0, hist, xy_out);
+        }
+        if (xy_out) {
+          cxy = xy_out;
+          cstride = 2;
         }
         PRT_CUDA(cudaGetLastError());
         return seg == n ? radix_sort_pairs<K>(kk0, v0, kk1, v1, n, 8 * (int)sizeof(K), sel, err, s, hist)
