@@ -472,6 +472,12 @@ struct TdLocalLevels {
   int count;
 };
 
+// The last level's runs (F records) are short: each record's new position in
+// its run is the number of the run's records with a smaller key, or an equal
+// key at an earlier position (a stable sort by counting), seg comparisons
+// per record instead of the radix passes.
+constexpr int kTdRankMax = 32;
+
 __device__ __forceinline__ int bit_length(uint32_t x) { return 32 - __clz(x); }
 __device__ __forceinline__ int bit_length(uint64_t x) { return 64 - __clzll((long long)x); }
 
@@ -505,6 +511,38 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) td_local_sort_ker
     const int seg = (int)min(lv.seg[level], (int64_t)kTdLocal);
     const int axis = lv.use_y[level];
     __syncthreads();
+    if (level == lv.count - 1 && seg <= kTdRankMax) {
+      // keys into the (x1, y1) array's space (no later level reads it)
+      K kq[kTdItems];
+#pragma unroll
+      for (int q = 0; q < kTdItems; q++) {
+        const int i = tid + 256 * q;
+        kq[q] = i < m ? (K)ukey(S.xy[S.item[cur][i] & 0xFFFFu][axis]) : K(0);
+      }
+      __syncthreads();
+      K *key = reinterpret_cast<K *>(&S.xy[0][0]);
+#pragma unroll
+      for (int q = 0; q < kTdItems; q++) {
+        const int i = tid + 256 * q;
+        if (i < m) key[i] = kq[q];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < kTdItems; q++) {
+        const int i = tid + 256 * q;
+        if (i < m) {
+          const int r0 = (i / seg) * seg, r1 = min(r0 + seg, m);
+          int rank = 0;
+          for (int j = r0; j < r1; j++) {
+            const K kj = key[j];
+            rank += (kj < kq[q] || (kj == kq[q] && j < i)) ? 1 : 0;
+          }
+          S.item[1 - cur][r0 + rank] = S.item[cur][i];
+        }
+      }
+      cur = 1 - cur;
+      continue;
+    }
     // the run of each item from its position in the order the previous level
     // left, and the tile's key range
     K lo = ~K(0), hi = 0;
