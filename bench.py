@@ -711,9 +711,9 @@ def overlay_e2e(prt, LA, LB, chunk_pairs: int = 1 << 20):
     host memory: both layers' arrays copied from pinned host memory to the
     device, polygon MBRs, bottom-up tree over layer A, join of layer B, and
     the batched clip streamed in chunks of `chunk_pairs` pairs
-    (prt.overlay_stream) whose results land in pinned host memory and are
-    copied into the caller's numpy arrays.  Wall time around it all, the
-    device synchronised at both ends."""
+    (prt.overlay_stream) whose results land in host memory, chunk by chunk,
+    and are handed to a callback (here it counts them).  Wall time around it
+    all, the device synchronised at both ends."""
     import psutil
     import torch
 

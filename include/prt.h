@@ -248,10 +248,11 @@ int prt_results_free(prt_results *r);
 /* Streaming overlay (no reference counterpart; the reference's results live
  * in a 1 GiB device heap, vector_map_overlay_gpc_kernel.cu:72): the pairs of
  * prt_overlay_run are clipped in chunks of at most chunk_pairs, and each
- * chunk's results are copied to pinned host memory in pair order and passed
- * to fn before their device memory is released, so device memory holds at
- * most two chunks' results however large the whole result set is.  A chunk's
- * copy-out overlaps the next chunk's clip.  fn receives the chunk's first
+ * chunk's results are copied to host memory in pair order and passed to fn
+ * (on the calling thread, in chunk order) once their device memory is
+ * released, so device memory holds at most two chunks' results however large
+ * the whole result set is.  A chunk's copy-out (a second host thread and
+ * stream, into two reused pageable buffers) overlaps the next chunk's clip.  fn receives the chunk's first
  * pair index and pair count and, valid only during the call, the CSR of
  * prt_results_copy (pair_cont_off [n+1] relative to the chunk, cont_nverts /
  * cont_hole per contour, xy as x, y pairs); a non-zero return stops the

@@ -324,8 +324,11 @@ def overlay_stream(pairs, base: Layer, over: Layer, fn, leaf_to_poly=None, offse
     """Clips the pairs in chunks of at most ``chunk_pairs`` (prt_overlay_stream):
     device memory holds at most two chunks' results.  For every chunk, in pair
     order, ``fn(first_pair, pair_cont_off, cont_nverts, cont_hole, xy)`` gets
-    numpy copies of its results (pair_cont_off relative to the chunk, xy
-    [V, 2]); a truthy return value stops the stream with an error."""
+    read-only numpy views of its results in host memory (pair_cont_off
+    relative to the chunk, xy [V, 2]), valid only during the call: copy what
+    must outlive it (a chunk is gigabytes at full size, and the library's
+    buffers are reused for the next chunk).  A truthy return value stops the
+    stream with an error."""
     p = _dev_tensor(pairs, torch.int32)
     l2p = _dev_tensor(leaf_to_poly, torch.int32) if leaf_to_poly is not None else None
     sb, so = base.struct(), over.struct()
@@ -333,12 +336,14 @@ def overlay_stream(pairs, base: Layer, over: Layer, fn, leaf_to_poly=None, offse
 
     def cb(user, first, n, off, nv, hole, xy):
         try:
-            o = np.ctypeslib.as_array(off, shape=(n + 1,)).copy()
+            o = np.ctypeslib.as_array(off, shape=(n + 1,))
             nc = int(o[-1])
-            nvv = np.ctypeslib.as_array(nv, shape=(max(nc, 1),))[:nc].copy()
-            hh = np.ctypeslib.as_array(hole, shape=(max(nc, 1),))[:nc].copy()
-            tv = int(nvv.sum())
-            xx = np.ctypeslib.as_array(xy, shape=(max(tv, 1), 2))[:tv].copy()
+            nvv = np.ctypeslib.as_array(nv, shape=(max(nc, 1),))[:nc] if nc else np.zeros(0, np.int32)
+            hh = np.ctypeslib.as_array(hole, shape=(max(nc, 1),))[:nc] if nc else np.zeros(0, np.int32)
+            tv = int(nvv.sum(dtype=np.int64))
+            xx = np.ctypeslib.as_array(xy, shape=(max(tv, 1), 2))[:tv] if tv else np.zeros((0, 2), np.float64)
+            for a in (o, nvv, hh, xx):
+                a.flags.writeable = False
             return 1 if fn(int(first), o, nvv, hh, xx) else 0
         except BaseException as e:  # surfaced after the C call returns
             err.append(e)

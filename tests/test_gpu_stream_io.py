@@ -34,7 +34,8 @@ def test_stream_equals_one_shot(cuda, sched, chunk):
     seen = []
 
     def take(first, o, n_, h_, x_):
-        seen.append((first, o, n_, h_, x_))
+        # the arrays are views valid only during the call
+        seen.append((first, o.copy(), n_.copy(), h_.copy(), x_.copy()))
         return 0
 
     prt.overlay_stream(pairs, LA, LB, take, leaf_to_poly=l2p, sched=sched, chunk_pairs=chunk)
