@@ -252,7 +252,9 @@ int prt_results_free(prt_results *r);
  * (on the calling thread, in chunk order) once their device memory is
  * released, so device memory holds at most two chunks' results however large
  * the whole result set is.  A chunk's copy-out (a second host thread and
- * stream, into two reused pageable buffers) overlaps the next chunk's clip.  fn receives the chunk's first
+ * stream, through two 256 MiB pinned buffers that the library keeps for the
+ * rest of the process, into two pageable buffers reused from chunk to chunk)
+ * overlaps the next chunk's clip.  fn receives the chunk's first
  * pair index and pair count and, valid only during the call, the CSR of
  * prt_results_copy (pair_cont_off [n+1] relative to the chunk, cont_nverts /
  * cont_hole per contour, xy as x, y pairs); a non-zero return stops the
