@@ -95,6 +95,32 @@ def test_topdown(cuda, kind, F, n):
     compare_bu(t.export_bu(), levels_to_bu(lv, F, perm))
 
 
+@pytest.mark.parametrize("kind", ["f32", "i64"])
+@pytest.mark.parametrize("F", [2, 4, 8])
+@pytest.mark.parametrize("n", [1, 5000, 40000])
+def test_small_fanouts(cuda, kind, F, n):
+    """Fanouts below 10: many short-run levels (at F=2 more than one
+    shared-memory launch holds), the last level's runs of F records sorted by
+    counting ranks; bottom-up and top-down both bit-exact against the oracle."""
+    import parlllelrtree_b200 as prt
+
+    b = boxes_of(kind, n, seed=11 * n + F)
+    perm = oracle.td_order(b, F)
+    lv = oracle.pack(b, F, perm)
+    t = prt.build_topdown(torch.from_numpy(b).cuda(), fanout=F)
+    check_levels(t, lv)
+    assert np.array_equal(t.leaf_order().cpu().numpy(), perm)
+    compare_td(t.export_td(), levels_to_td(lv, F))
+    modes = [("morton32", oracle.keys_morton32(b)[0])]
+    if kind == "i64":
+        modes.append(("ref64", oracle.keys_ref64(b)[0]))
+    for mode, keys in modes:
+        perm_bu = oracle.stable_argsort(keys)
+        tb = prt.build_bottomup(torch.from_numpy(b).cuda(), fanout=F, key_mode=mode)
+        assert np.array_equal(tb.leaf_order().cpu().numpy(), perm_bu)
+        check_levels(tb, oracle.pack(b, F, perm_bu))
+
+
 def test_sort_stability_many_ties(cuda):
     """Heavy key ties: the leaf order must keep input order inside each tie."""
     import parlllelrtree_b200 as prt
