@@ -135,13 +135,17 @@ def fit_affine(A: dict, B: dict, steps: int = 200, stages=((30, 50), (10, 50), (
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record()
         stage_rec, stage_ov = [], []
+        cap = None  # pair capacity: the previous step's count plus a margin
         for it in range(k_steps):
             opt.zero_grad()
             xb = _dilate(_apply(theta, xb_all[vi]), rv, owner, float(stride))
             LB.xy = xb.detach().contiguous()
             # every step: R-tree over the moved layer's MBRs, join, clip, adjoint
             tree = prt.build_bottomup(LB.mbr(), fanout=fanout)
-            pairs = tree.join(qa)
+            # one traversal when the capacity suffices (the join reports the
+            # count and is re-run only when it does not)
+            pairs = tree.join(qa, cap=cap)
+            cap = len(pairs) + len(pairs) // 4 + 1024
             pb = tree.leaf_order()[pairs[:, 0].long()]
             pa = pairs[:, 1].contiguous()
             area = prt.intersection_area(LA, LB, pa, pb, base_xy=LA.xy, over_xy=xb)
