@@ -27,7 +27,10 @@ constexpr int kSortWarps = kSortBlock / 32;
 #define PRT_SORT_ITEMS 16  // keys per thread of a tile
 #endif
 #ifndef PRT_SORT_MIN_BLOCKS
-#define PRT_SORT_MIN_BLOCKS 3  // resident blocks per SM the pass is compiled for
+// resident blocks per SM the pass is compiled for: 4 (64 registers, a 56-byte
+// spill) against 3 (80 registers): 0.0872 -> 0.0830-0.0840 ms per 10M-key
+// pass, measured with the look-back batch below
+#define PRT_SORT_MIN_BLOCKS 4
 #endif
 constexpr int kItems = PRT_SORT_ITEMS;
 constexpr int kTile = kSortBlock * kItems;
@@ -122,7 +125,7 @@ struct PassSmem {
 };
 
 #ifndef PRT_SORT_LOOKBATCH
-#define PRT_SORT_LOOKBATCH 8
+#define PRT_SORT_LOOKBATCH 4  // 2, 4, 8, 16 measured: 4 best at 4 blocks per SM
 #endif
 #ifndef PRT_SORT_BACKOFF_NS
 #define PRT_SORT_BACKOFF_NS 0  // pause between look-back polls that found nothing new
