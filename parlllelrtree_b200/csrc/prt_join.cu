@@ -137,29 +137,45 @@ __global__ void __launch_bounds__(kJoinBlock) expand_kernel(JoinLevel J, const B
   }
 }
 
+// Resident blocks per SM of expand_kernel<T, G> (once per instantiation): the
+// grid is exactly one wave, since a block beyond it would process its share
+// of every grid-stride loop after the others.
+template <typename T, int G>
+int expand_blocks() {
+  static std::atomic<int> per_sm{0};
+  int b = per_sm.load(std::memory_order_relaxed);
+  if (b == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, expand_kernel<T, G>, kJoinBlock, 0) != cudaSuccess || b < 1) {
+      cudaGetLastError();
+      b = 4;
+    }
+    per_sm.store(b, std::memory_order_relaxed);
+  }
+  return kSMs * b;
+}
+
 template <typename T>
 int launch_expand(const JoinLevel &J, const void *queries, int fanout, cudaStream_t s) {
   const Box<T> *q = reinterpret_cast<const Box<T> *>(queries);
-  int blocks = kSMs * 8;
   if (fanout <= 2) {
     PRT_PROF("expand", s);
-    expand_kernel<T, 2><<<blocks, kJoinBlock, 0, s>>>(J, q, fanout);
+    expand_kernel<T, 2><<<expand_blocks<T, 2>(), kJoinBlock, 0, s>>>(J, q, fanout);
   }
   else if (fanout <= 4) {
     PRT_PROF("expand", s);
-    expand_kernel<T, 4><<<blocks, kJoinBlock, 0, s>>>(J, q, fanout);
+    expand_kernel<T, 4><<<expand_blocks<T, 4>(), kJoinBlock, 0, s>>>(J, q, fanout);
   }
   else if (fanout <= 8) {
     PRT_PROF("expand", s);
-    expand_kernel<T, 8><<<blocks, kJoinBlock, 0, s>>>(J, q, fanout);
+    expand_kernel<T, 8><<<expand_blocks<T, 8>(), kJoinBlock, 0, s>>>(J, q, fanout);
   }
   else if (fanout <= 16) {
     PRT_PROF("expand", s);
-    expand_kernel<T, 16><<<blocks, kJoinBlock, 0, s>>>(J, q, fanout);
+    expand_kernel<T, 16><<<expand_blocks<T, 16>(), kJoinBlock, 0, s>>>(J, q, fanout);
   }
   else {
     PRT_PROF("expand", s);
-    expand_kernel<T, 32><<<blocks, kJoinBlock, 0, s>>>(J, q, fanout);
+    expand_kernel<T, 32><<<expand_blocks<T, 32>(), kJoinBlock, 0, s>>>(J, q, fanout);
   }
   return PRT_OK;
 }
