@@ -44,8 +44,8 @@ struct JoinLevel {
 // frontier items of all rounds are loaded first, then their node entries, so
 // each warp has that many independent loads in flight; the hits of the whole
 // iteration are reserved with one atomicAdd per block.  Measured on the
-// 1M-window join of the 10M-box tree (F = 16): 1, 2, 3, 4, 6, 8 rounds take
-// 4.80, 3.47, 3.00, 4.32, 4.02, 3.81 ms.
+// 1M-window join of the 10M-box tree (F = 16) with the grid sized to one
+// resident wave: 3, 4, 6 rounds take 3.00, 3.29, 3.07 ms.
 constexpr int kJoinRounds = 3;
 
 template <typename T, int G>
