@@ -432,15 +432,16 @@ __global__ void select_copy_u32_kernel(const uint32_t *a, const uint32_t *b, con
 // levels of the build: run lengths F^k <= 4096, each dividing the one before)
 // are sorted together, tile by tile, in shared memory: one CTA takes as many
 // whole runs of the first such level as fit in a tile of kTdLocal records (in
-// the current order), and for each level in turn gathers each record's
-// coordinate key (the first level's gather leaves the tile's boxes in L2 for
-// the later ones) and sorts the tile stably by (run within the tile, key)
-// with an LSD radix sort in shared memory, 8 bits per pass, each pass ranked
-// by the warp multisplit (lanes with the same digit from one ballot per digit
-// bit).  The tile's index order is the current order, so equal keys keep it,
-// as each level's stable sort requires; each item's run is carried along the
-// passes.  One read and one write of the order replace 4-7 global passes per
-// level.
+// the current order), gathers each record's (x1, y1) once, and sorts the tile
+// level by level.  A level with runs longer than F sorts stably by (run
+// within the tile, key - the tile's smallest key) with an LSD radix sort in
+// shared memory over only the bits that needs, 8 bits per pass, each pass
+// ranked by the warp multisplit (lanes with the same digit from one ballot
+// per digit bit); the last level (runs of F <= 32) places each record by
+// counting the run's smaller keys.  The tile's index order is the current
+// order, so equal keys keep it, as each level's stable sort requires; each
+// item's run travels with it.  One read and one write of the order replace
+// 4-7 global passes per level.
 constexpr int kTdLocal = 4096;
 constexpr int kTdItems = kTdLocal / 256;  // per thread (256 threads)
 constexpr int kTdMaxLocal = 12;           // local levels one launch sorts (4096 = 2^12)
