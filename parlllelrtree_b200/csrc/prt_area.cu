@@ -4,7 +4,7 @@
 // over the pieces of A's edges inside B and of B's edges inside A, found by
 // the same slab / parity pass as the adjoint below (area mode).  Pairs whose
 // crossings are not all clean, whose polygons do not fit the shared-memory
-// staging, or whose area the crossing-rounding bound does not pin to 1e-11 are
+// staging, or whose area the crossing-rounding bound does not pin to 1e-10 are
 // clipped by GPC instead (prt_overlay.cu, area-only mode: the clip result is
 // reduced to its shoelace area in place and never written out).  The fast
 // path assumes what GPC's output implies for map layers: the rings of a
@@ -21,8 +21,14 @@
 //     d area / d p += N sum ((t1 - t0) - (t1^2 - t0^2) / 2)
 // One warp per pair: lanes take edges of A (then of B); each lane finds its
 // edge's crossings with the other polygon, in increasing t, and classifies
-// each interval by an even-odd test of its midpoint.  Contributions are scaled by the upstream gradient and
-// accumulated with atomicAdd, since a polygon may appear in many pairs.
+// the intervals between them (by crossing parity along the ring, or by the
+// even-odd test of each midpoint when a crossing is not clean; see
+// pair_boundary).  Contributions are scaled by the upstream gradient and
+// accumulated with atomicAdd, since a polygon may appear in many pairs.  Both
+// directions run in two stages: polygons of up to 64 vertices staged in
+// shared memory first, the pairs that do not fit listed for a 128-vertex
+// staging, larger ones on a global-memory path (backward) or the GPC clip
+// (forward).
 #include <cuda_runtime.h>
 
 #include <atomic>
