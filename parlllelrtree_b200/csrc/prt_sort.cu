@@ -27,9 +27,10 @@ constexpr int kSortWarps = kSortBlock / 32;
 #define PRT_SORT_ITEMS 16  // keys per thread of a tile
 #endif
 #ifndef PRT_SORT_MIN_BLOCKS
-// resident blocks per SM the pass is compiled for: 4 (64 registers, a 56-byte
-// spill) against 3 (80 registers): 0.0872 -> 0.0830-0.0840 ms per 10M-key
-// pass, measured with the look-back batch below
+// resident blocks per SM the 32-bit-key pass is compiled for: 4 (64
+// registers, a 56-byte spill) against 3 (80 registers): 0.0872 ->
+// 0.0830-0.0840 ms per 10M-key pass, measured with the look-back batch below.
+// The 64-bit-key pass stays at 3: its 58 KB tile fits no more per SM.
 #define PRT_SORT_MIN_BLOCKS 4
 #endif
 constexpr int kItems = PRT_SORT_ITEMS;
@@ -133,7 +134,7 @@ struct PassSmem {
 constexpr int kLookBatch = PRT_SORT_LOOKBATCH;  // predecessor statuses read per look-back step
 
 template <typename KeyT>
-__global__ void __launch_bounds__(kSortBlock, PRT_SORT_MIN_BLOCKS) onesweep_pass(KeyT *keys0, uint32_t *vals0, KeyT *keys1,
+__global__ void __launch_bounds__(kSortBlock, sizeof(KeyT) == 4 ? PRT_SORT_MIN_BLOCKS : 3) onesweep_pass(KeyT *keys0, uint32_t *vals0, KeyT *keys1,
                                                            uint32_t *vals1, int64_t n, int shift,
                                                            const PassPlan *__restrict__ plan,
                                                            const uint32_t *__restrict__ goff,
