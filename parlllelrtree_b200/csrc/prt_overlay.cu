@@ -755,7 +755,6 @@ __global__ void graph_bins_kernel(const uint32_t *__restrict__ k0, const uint32_
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const uint32_t *k = *sel ? k1 : k0;
   const int64_t count = (int64_t)min((unsigned long long)cap, *d_count);
-  int64_t lo_prev = 0;
   for (int b = 0; b < nbins; b++) {
     int64_t lo = 0, hi = count;
     while (lo < hi) {
@@ -766,10 +765,8 @@ __global__ void graph_bins_kernel(const uint32_t *__restrict__ k0, const uint32_
     }
     if (b > 0) ranges[2 * (b - 1) + 1] = lo;
     ranges[2 * b] = lo;
-    lo_prev = lo;
   }
   ranges[2 * (nbins - 1) + 1] = count;
-  (void)lo_prev;
 }
 
 __global__ void graph_totals_kernel(const int64_t *__restrict__ pair_cstart, const int32_t *__restrict__ pair_ncont,
@@ -1222,7 +1219,6 @@ int prt_clip_pair_host(int op, int s_ncont, const int32_t *s_nverts, const doubl
   PRT_CHECK(out_ncont && out_nv && (s_ncont == 0 || (s_nverts && s_xy)) && (c_ncont == 0 || (c_nverts && c_xy)),
             PRT_ERR_INVALID, "NULL argument");
   PRT_CHECK(s_ncont >= 0 && c_ncont >= 0, PRT_ERR_INVALID, "negative contour count");
-  cudaStream_t s = 0;
   // layers with one polygon each (zero-ring polygons allowed)
   std::vector<int64_t> pr_s = {0, s_ncont}, pr_c = {0, c_ncont};
   std::vector<int64_t> rv_s(s_ncont + 1, 0), rv_c(c_ncont + 1, 0);
@@ -1266,7 +1262,6 @@ int prt_clip_pair_host(int op, int s_ncont, const int32_t *s_nverts, const doubl
   cudaFree(d_i64);
   cudaFree(d_xy);
   cudaFree(d_pair);
-  (void)s;
   return rc;
 }
 
