@@ -443,7 +443,15 @@ __global__ void select_copy_u32_kernel(const uint32_t *a, const uint32_t *b, con
 // item's run travels with it.  One read and one write of the order replace
 // 4-7 global passes per level.
 constexpr int kTdLocal = 4096;
-constexpr int kTdItems = kTdLocal / 256;  // per thread (256 threads)
+#ifndef PRT_TD_THREADS
+// 512 threads of 8 records (64 registers, 2 CTAs of 16 warps per SM) against
+// 256 of 16 (80 registers with a spill, 3 CTAs of 8 warps): the top-down
+// build of 10M boxes (F = 16) 2.18 -> 2.07 ms
+#define PRT_TD_THREADS 512
+#endif
+constexpr int kTdThreads = PRT_TD_THREADS;     // per CTA
+constexpr int kTdWarps = kTdThreads / 32;
+constexpr int kTdItems = kTdLocal / kTdThreads;  // per thread
 constexpr int kTdMaxLocal = 12;           // local levels one launch sorts (4096 = 2^12)
 
 __device__ __forceinline__ uint32_t lane_lt() {
@@ -460,10 +468,10 @@ template <typename T>
 struct TdLocalSmem {
   uint32_t item[2][kTdLocal];
   T xy[kTdLocal][2];
-  uint32_t wh[8][256];
+  uint32_t wh[kTdWarps][256];
   uint32_t dstart[256];
   uint32_t wsum[8];
-  unsigned long long red[2][8];
+  unsigned long long red[2][kTdWarps];
 };
 
 // The local levels, in order: run length and axis (0: x1, 1: y1) of each.
@@ -488,7 +496,8 @@ __device__ __forceinline__ int bit_length(uint64_t x) { return 64 - __clzll((lon
 // from every key keeps their order, so this is the order of a stable sort by
 // key within each run.
 template <typename T, int kStride>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) td_local_sort_kernel(
+__global__ void __launch_bounds__(kTdThreads, kTdThreads == 256 ? (sizeof(T) == 4 ? 3 : 2) : (sizeof(T) == 4 ? 2 : 1))
+    td_local_sort_kernel(
     const T *__restrict__ c, const uint32_t *__restrict__ perm_a, const uint32_t *__restrict__ perm_b,
     const int *__restrict__ sel, int64_t n, TdLocalLevels lv, uint32_t *__restrict__ perm_out) {
   using K = typename std::conditional<sizeof(T) == 8, uint64_t, uint32_t>::type;
@@ -499,7 +508,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) td_local_sort_ker
   const int64_t base = blockIdx.x * chunk;
   const int m = (int)min(chunk, n - base);
   const uint32_t *perm_in = cur_perm(perm_a, perm_b, sel);
-  for (int i = tid; i < m; i += 256) {
+  for (int i = tid; i < m; i += kTdThreads) {
     uint32_t r = perm_in ? perm_in[base + i] : (uint32_t)(base + i);
     if ((int64_t)r >= n) r = 0;  // only after a timed-out sort (reported by the caller)
     S.xy[i][0] = __ldg(&c[kStride * (int64_t)r]);
@@ -517,20 +526,20 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) td_local_sort_ker
       K kq[kTdItems];
 #pragma unroll
       for (int q = 0; q < kTdItems; q++) {
-        const int i = tid + 256 * q;
+        const int i = tid + kTdThreads * q;
         kq[q] = i < m ? (K)ukey(S.xy[S.item[cur][i] & 0xFFFFu][axis]) : K(0);
       }
       __syncthreads();
       K *key = reinterpret_cast<K *>(&S.xy[0][0]);
 #pragma unroll
       for (int q = 0; q < kTdItems; q++) {
-        const int i = tid + 256 * q;
+        const int i = tid + kTdThreads * q;
         if (i < m) key[i] = kq[q];
       }
       __syncthreads();
 #pragma unroll
       for (int q = 0; q < kTdItems; q++) {
-        const int i = tid + 256 * q;
+        const int i = tid + kTdThreads * q;
         if (i < m) {
           const int r0 = (i / seg) * seg, r1 = min(r0 + seg, m);
           int rank = 0;
@@ -547,7 +556,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) td_local_sort_ker
     // the run of each item from its position in the order the previous level
     // left, and the tile's key range
     K lo = ~K(0), hi = 0;
-    for (int i = tid; i < m; i += 256) {
+    for (int i = tid; i < m; i += kTdThreads) {
       const uint32_t slot = S.item[cur][i] & 0xFFFFu;
       S.item[cur][i] = (uint32_t)(i / seg) << 16 | slot;
       const K k = (K)ukey(S.xy[slot][axis]);
@@ -565,7 +574,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) td_local_sort_ker
     }
     __syncthreads();
 #pragma unroll
-    for (int w = 0; w < 8; w++) {
+    for (int w = 0; w < kTdWarps; w++) {
       const K a = (K)S.red[0][w], z = (K)S.red[1][w];
       lo = a < lo ? a : lo;
       hi = z > hi ? z : hi;
@@ -577,7 +586,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) td_local_sort_ker
     for (int shift = 0; shift < total_bits; shift += 8) {
       const int width = min(8, total_bits - shift);
       __syncthreads();
-      for (int i = tid; i < 8 * 256; i += 256) (&S.wh[0][0])[i] = 0;
+      for (int i = tid; i < kTdWarps * 256; i += kTdThreads) (&S.wh[0][0])[i] = 0;
       __syncthreads();
       uint32_t it[kTdItems];
       int dg[kTdItems];
@@ -624,26 +633,31 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) td_local_sort_ker
         __syncwarp();
       }
       __syncthreads();
-      // thread d: exclusive prefix of digit d over the warps, then over digits
-      uint32_t tot = 0;
+      // thread d < 256: exclusive prefix of digit d over the warps, then over
+      // digits (warps 0-7; the others wait at the barriers)
+      uint32_t tot = 0, incl = 0;
+      if (tid < 256) {
 #pragma unroll
-      for (int w = 0; w < 8; w++) {
-        const uint32_t x = S.wh[w][tid];
-        S.wh[w][tid] = tot;
-        tot += x;
-      }
-      uint32_t incl = tot;
+        for (int w = 0; w < kTdWarps; w++) {
+          const uint32_t x = S.wh[w][tid];
+          S.wh[w][tid] = tot;
+          tot += x;
+        }
+        incl = tot;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += y;
+        }
+        if (lane == 31) S.wsum[warp] = incl;
       }
-      if (lane == 31) S.wsum[warp] = incl;
       __syncthreads();
-      uint32_t woff = 0;
+      if (tid < 256) {
+        uint32_t woff = 0;
 #pragma unroll
-      for (int w = 0; w < 8; w++) woff += w < warp ? S.wsum[w] : 0u;
-      S.dstart[tid] = woff + incl - tot;
+        for (int w = 0; w < 8; w++) woff += w < warp ? S.wsum[w] : 0u;
+        S.dstart[tid] = woff + incl - tot;
+      }
       __syncthreads();
 #pragma unroll
       for (int j = 0; j < kTdItems; j++) {
@@ -654,7 +668,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) td_local_sort_ker
     }
   }
   __syncthreads();
-  for (int i = tid; i < m; i += 256) {
+  for (int i = tid; i < m; i += kTdThreads) {
     const uint32_t slot = S.item[cur][i] & 0xFFFFu;
     uint32_t r = perm_in ? perm_in[base + slot] : (uint32_t)(base + slot);
     if ((int64_t)r >= n) r = 0;
@@ -681,9 +695,9 @@ int td_local_levels(const T *cxy, int stride, const uint32_t *perm_a, const uint
   {
     PRT_PROF("td_local_sort", s);
     if (stride == 2)
-      td_local_sort_kernel<T, 2><<<(unsigned)blocks, 256, smem, s>>>(cxy, perm_a, perm_b, sel, n, lv, perm_out);
+      td_local_sort_kernel<T, 2><<<(unsigned)blocks, kTdThreads, smem, s>>>(cxy, perm_a, perm_b, sel, n, lv, perm_out);
     else
-      td_local_sort_kernel<T, 4><<<(unsigned)blocks, 256, smem, s>>>(cxy, perm_a, perm_b, sel, n, lv, perm_out);
+      td_local_sort_kernel<T, 4><<<(unsigned)blocks, kTdThreads, smem, s>>>(cxy, perm_a, perm_b, sel, n, lv, perm_out);
   }
   PRT_CUDA(cudaGetLastError());
   return PRT_OK;
